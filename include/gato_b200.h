@@ -1,0 +1,242 @@
+/*
+ * gato_b200 — C ABI of the batched SQP trajectory-optimisation solver for
+ * NVIDIA B200 (sm_100a).
+ *
+ * This header is the drop-in boundary for the reference's pybind11 module
+ * `bsqpN{N}_{plant}` (python/bindings.cu) and the solver class it wraps
+ * (gato/bsqp/bsqp.cuh).  Every entry point below names the reference
+ * interface it replaces.  The ABI uses plain C types only: pointers, sizes,
+ * int status codes.  No C++ or torch types cross it.
+ *
+ * Conventions
+ *   - n = 2*nq (state size), m = nq (control size), N knots, B problems.
+ *   - XU trajectory per problem: [x_0 u_0 x_1 u_1 ... x_{N-1}], length
+ *     (n+m)*N - m (gato/utils/linalg.cuh:624-634).
+ *   - goal per problem: 6 floats per knot [px py pz r p y]; only xyz is used.
+ *   - lambda per problem: (N+2)*n floats, one zero block padding each end
+ *     (gato/utils/linalg.cuh:648-660).
+ *   - Functions taking `d_` pointers expect device memory; `h_` pointers are
+ *     host memory.  All return GATO_OK (0) or a negative error code;
+ *     gato_last_error() gives the message of the last failure on the calling
+ *     thread.
+ *   - A solver handle is bound to the CUDA device that was current when it was
+ *     created.  Calls on one handle must not overlap; distinct handles are
+ *     independent.
+ */
+#ifndef GATO_B200_H
+#define GATO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GATO_MAX_NQ 8
+
+enum {
+    GATO_OK = 0,
+    GATO_ERR_ARG = -1,       /* invalid argument (size, pointer, enum) */
+    GATO_ERR_CUDA = -2,      /* a CUDA runtime call failed */
+    GATO_ERR_UNSUPPORTED = -3,
+    GATO_ERR_NOMEM = -4,
+    GATO_ERR_TIMEOUT = -5    /* a bounded device wait expired */
+};
+
+enum { GATO_PLANT_IIWA14 = 0, GATO_PLANT_INDY7 = 1 };
+
+/* Solver forms.  Both run the same SQP method with the same batch semantics. */
+enum {
+    GATO_FORM_PLAIN = 0,  /* one kernel per stage, host convergence check per
+                             SQP iteration (the reference's driver shape) */
+    GATO_FORM_FUSED = 1   /* one persistent kernel per SQP stage group, device
+                             side convergence, whole solve in a CUDA graph */
+};
+
+/* Arithmetic of the device path. */
+enum {
+    GATO_PREC_FP32 = 0,   /* everything FP32 (the reference's arithmetic) */
+    GATO_PREC_MIXED = 1   /* FP32 math, FP64 PCG inner products, alpha/beta
+                             recurrences and merit reductions */
+};
+
+/*
+ * Robot description: a serial chain of revolute joints, each rotating about
+ * the z axis of its joint frame (URDF <axis xyz="0 0 1"/>).  Joint i's frame is
+ * placed in link i-1's frame by (joint_xyz, joint_rpy) exactly as the URDF
+ * <origin> tag.  Up to two rigid bodies are fixed to each link (a link plus a
+ * fixed child such as a flange); mass 0 marks an unused slot.
+ * Replaces the compile-time GRiD tables of gato/dynamics/{iiwa14,indy7}/
+ * *_grid.cuh (init_XImats, iiwa14_grid.cuh:1210-2098) and the limit tables of
+ * gato/dynamics/iiwa14/iiwa14_plant.cuh:37-88.
+ */
+typedef struct gato_model {
+    int nq;
+    double joint_xyz[GATO_MAX_NQ][3];
+    double joint_rpy[GATO_MAX_NQ][3];
+    /* per link, per body: mass, com x y z, ixx ixy ixz iyy iyz izz (about the
+       com, in the link frame's axes) */
+    double link_inertial[GATO_MAX_NQ][2][10];
+    double q_limit[GATO_MAX_NQ];   /* |q| limit (symmetric)   */
+    double qd_limit[GATO_MAX_NQ];  /* |qd| limit (symmetric)  */
+    double u_limit[GATO_MAX_NQ];   /* |u| limit (symmetric)   */
+    double limit_margin;           /* added to the upper limit, subtracted from
+                                      the lower: -0.1 tightens by 0.1 */
+    double gravity;                /* 9.81 */
+    int barrier_style;             /* 0: exact diagonal barrier Hessian
+                                        (iiwa14_plant.cuh:113-155)
+                                     1: outer product of barrier gradients
+                                        (indy7_plant.cuh:141-147, 385-415) */
+} gato_model_t;
+
+/* Solver settings; the field meaning follows the BSQP constructor
+   (gato/bsqp/bsqp.cuh:43-59, python/bsqp/interface.py:7-32). */
+typedef struct gato_params {
+    double dt;
+    int max_sqp_iters;
+    double kkt_tol;          /* accepted for interface parity; unused by the
+                                method, as in bsqp.cuh:153 */
+    int max_pcg_iters;
+    double pcg_tol;
+    double solve_ratio;
+    double mu;
+    double q_cost;
+    double qd_cost;
+    double u_cost;
+    double N_cost;
+    double q_lim_cost;
+    double vel_lim_cost;
+    double ctrl_lim_cost;
+    double rho;
+} gato_params_t;
+
+/* Per-solve statistics, all host memory supplied by the caller; any pointer
+   may be NULL.  Replaces the dict built in python/bindings.cu:96-147.
+   Arrays indexed [iteration][problem] hold max_sqp_iters*B entries; the first
+   ls_num_iters rows are valid. */
+typedef struct gato_stats {
+    double sqp_time_us;      /* device time of the solve (CUDA events) */
+    int ls_num_iters;        /* SQP iterations that ran the line search */
+    int32_t* sqp_iters;      /* [B] */
+    int32_t* kkt_converged;  /* [B] */
+    float* final_merit;      /* [B] */
+    float* initial_merit;    /* [B] */
+    int32_t* pcg_iters;      /* [max_sqp_iters][B] */
+    float* ls_min_merit;     /* [max_sqp_iters][B] */
+    float* ls_step_size;     /* [max_sqp_iters][B] */
+} gato_stats_t;
+
+typedef struct gato_solver gato_solver_t;
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* gato_last_error(void);
+
+/* Version string of the library. */
+const char* gato_version(void);
+
+/* Fills *out with a built-in robot.  Replaces the compile-time plant choice
+   PLANT_IIWA14 / PLANT_INDY7 (gato/settings.h:35-41). */
+int gato_builtin_model(int plant, gato_model_t* out);
+
+/* Creates a solver for `batch` problems of horizon N on the current device.
+   Replaces BSQP<T,B>::BSQP (gato/bsqp/bsqp.cuh:43-59) and PyBSQP::PyBSQP
+   (python/bindings.cu:27-56); N and batch are runtime values here
+   (2 <= N <= 256, 1 <= batch <= 65536).  `form` is a GATO_FORM_* value and
+   `precision` a GATO_PREC_* value. */
+int gato_create(const gato_model_t* model, int N, int batch,
+                const gato_params_t* params, int form, int precision,
+                gato_solver_t** out);
+
+/* Frees the solver and its device memory.  Replaces BSQP::~BSQP
+   (bsqp.cuh:61, 258-297). */
+void gato_destroy(gato_solver_t* s);
+
+/* Sizes of the solver's per-problem vectors (floats). */
+int gato_sizes(const gato_solver_t* s, int* nx, int* nu, int* traj_size,
+               int* goal_size, int* lambda_size);
+
+/* Runs the SQP solve on device buffers, stream-ordered on `stream`
+   (a cudaStream_t, 0 = legacy default stream).  d_xu [B][traj] is updated in
+   place; d_xs [B][nx] is the initial state; d_goal [B][6N] the end-effector
+   goals.  Statistics are copied into *stats (may be NULL); when stats is
+   non-NULL the call synchronises the stream before returning.
+   Replaces BSQP<T,B>::solve (gato/bsqp/bsqp.cuh:103-197). */
+int gato_solve(gato_solver_t* s, void* stream, float* d_xu, const float* d_xs,
+               const float* d_goal, gato_stats_t* stats);
+
+/* Same solve from host buffers: copies the inputs in, solves and copies XU
+   back into h_xu.  Replaces PyBSQP::solve (python/bindings.cu:68-148). */
+int gato_solve_host(gato_solver_t* s, float* h_xu, float dt, const float* h_xs,
+                    const float* h_goal, gato_stats_t* stats);
+
+/* Batched setters (host arrays of B floats, or 6*B for f_ext).
+   Replace BSQP::set_f_ext_batch / set_rho_penalty_batch / set_drho_batch /
+   set_mu_batch / set_pcg_tol_batch (gato/bsqp/bsqp.cuh:63-83) and their
+   bindings (python/bindings.cu:150-178). */
+int gato_set_f_ext_batch(gato_solver_t* s, const float* h_f_ext);
+int gato_set_rho_penalty_batch(gato_solver_t* s, const float* h_rho,
+                               int set_as_reset_default);
+int gato_set_drho_batch(gato_solver_t* s, const float* h_drho,
+                        int set_as_reset_default);
+int gato_set_mu_batch(gato_solver_t* s, const float* h_mu);
+int gato_set_pcg_tol_batch(gato_solver_t* s, const float* h_tol);
+
+/* Sets the time step used by gato_solve (gato_solve_host takes it per call,
+   as PyBSQP::solve does). */
+int gato_set_dt(gato_solver_t* s, float dt);
+
+/* Zeroes the dual warm start.  Replaces BSQP::reset_dual (bsqp.cuh:85). */
+int gato_reset_dual(gato_solver_t* s);
+/* Restores rho and drho to their reset defaults.  Replaces BSQP::reset_rho
+   (bsqp.cuh:87-91). */
+int gato_reset_rho(gato_solver_t* s);
+/* Enables/disables rho adaptation.  Replaces BSQP::set_rho_adaptation
+   (bsqp.cuh:93). */
+int gato_set_rho_adaptation(gato_solver_t* s, int enabled);
+
+/* Copies the dual warm start lambda [B][(N+2)*nx] out of / into the solver
+   (host memory).  The reference keeps it device-internal (bsqp.cuh:81). */
+int gato_get_lambda(gato_solver_t* s, float* h_lambda);
+int gato_set_lambda(gato_solver_t* s, const float* h_lambda);
+/* Copies the current penalty rho [B] out (host memory). */
+int gato_get_rho(gato_solver_t* s, float* h_rho);
+
+/* One integrator step of every problem from the same (x_k, u_k) under each
+   problem's own f_ext: h_xkp1 [B][nx] from h_xk [nx], h_uk [nu].
+   Replaces BSQP::sim_forward / PyBSQP::sim_forward (bsqp.cuh:95,
+   python/bindings.cu:180-194, gato/bsqp/kernels/sim.cuh:14-86). */
+int gato_sim_forward(gato_solver_t* s, const float* h_xk, const float* h_uk,
+                     float dt, float* h_xkp1);
+
+/*
+ * Stage-level entry points on device buffers, for parity testing and custom
+ * drivers.  Layouts follow the reference's batch layouts:
+ *   Q [B][N][n*n], R [B][N][m*m], q [B][N][n], r [B][N][m], A [B][N][n*n],
+ *   B [B][N][n*m], c [B][N][n] (column-major blocks, gato/types.cuh:65-73);
+ *   S, Pinv [B][N][3*n*n] row-major block rows; gamma [B][(N+2)*n].
+ */
+/* Replaces setupKKTSystemBatched (gato/bsqp/kernels/setup_kkt.cuh:130-157). */
+int gato_stage_setup_kkt(gato_solver_t* s, void* stream, const float* d_xu,
+                         const float* d_xs, const float* d_goal, float* d_Q,
+                         float* d_R, float* d_q, float* d_r, float* d_A,
+                         float* d_B, float* d_c);
+/* Replaces formSchurSystemBatched (gato/bsqp/kernels/schur_linsys.cuh:295-308).
+   Reads Q,R,q,r,A,B,c; writes S, Pinv, gamma, and overwrites d_Q/d_R with
+   the inverses (Q+rho*I_q)^-1 and R^-1 as the reference does. */
+int gato_stage_form_schur(gato_solver_t* s, void* stream, float* d_Q,
+                          float* d_R, const float* d_q, const float* d_r,
+                          const float* d_A, const float* d_B,
+                          const float* d_c, float* d_S, float* d_Pinv,
+                          float* d_gamma);
+/* Replaces solvePCGBatched (gato/bsqp/kernels/pcg.cuh:157-166).  d_lambda is
+   the warm start in, solution out; d_iters [B] receives iteration counts. */
+int gato_stage_pcg(gato_solver_t* s, void* stream, const float* d_S,
+                   const float* d_Pinv, const float* d_gamma, float* d_lambda,
+                   int32_t* d_iters);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GATO_B200_H */
