@@ -1,0 +1,453 @@
+#!/usr/bin/env python
+"""Benchmark: batched SQP solves/s on one B200 (replicas on N GPUs).
+
+Workload (one "step" = one batched solve): iiwa14, N=32 knots, dt=0.01 s,
+batch 1024 problems per GPU, seeded figure-8 end-effector goals, warm-started
+from a perturbed converged solution (XU and lambda), 5 SQP iterations, PCG
+max 173 iterations at tol 1e-5, FP32, cost weights at the reference interface
+defaults.  Each timed step starts from the same warm start (the solver's
+persistent lambda / rho are restored between steps, outside the timed region),
+and L2 is flushed between steps.
+
+  value     solves/s of the fused CUDA-graph form, inputs resident in HBM
+  e2e       solves/s through gato_solve_host (host buffers; H2D of XU, x0,
+            goals and D2H of XU inside the timed region)
+  plain     solves/s of the plain per-kernel form, same workload
+  roofline  FP32 CUDA-core roofline of the dominant kernel (k_fused_iter)
+  cpu_baseline  the FP64 oracle of the same SQP on the host cores, bounded
+            sample of the same workload
+
+`--impl reference` times the reference's algorithm on the host CPU (the FP64
+oracle port: the reference's solver has no CPU implementation and its CUDA
+kernels do not compile for the host) on a bounded sample per step.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PLANT, N, DT = "iiwa14", 32, 0.01
+SQP_ITERS, PCG_MAX, PCG_TOL = 5, 173, 1e-5
+METRIC = "SQP solves/s (iiwa14 N=32, batch 1024, 5 SQP iters, PCG tol 1e-5)"
+WORKLOAD = ("iiwa14 N=32 dt=0.01, batch 1024 per GPU, seeded figure-8 goals, perturbed "
+            "converged warm start, 5 SQP iters, PCG max 173 tol 1e-5, interface-default costs")
+
+
+def solver_kwargs():
+    # BSQP interface defaults (python/bsqp/interface.py:13-26) with the
+    # workload's iteration limits
+    return dict(max_sqp_iters=SQP_ITERS, max_pcg_iters=PCG_MAX, pcg_tol=PCG_TOL, kkt_tol=1e-4,
+                solve_ratio=1.0, mu=1.0, q_cost=2.0, qd_cost=1e-4, u_cost=1e-6, N_cost=50.0,
+                q_lim_cost=1e-3, vel_lim_cost=0.0, ctrl_lim_cost=0.0, rho=0.0)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=1024)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed"])
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="problems in the CPU baseline sample (0: sized to ~10 s)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------
+def make_workload(batch, seed):
+    """Synthetic inputs plus a warm start: the fused solver run to
+    convergence from the default warm start, perturbed by seeded noise."""
+    import gato_b200
+    from gato_b200 import workloads as W
+    pr = W.make_problem(PLANT, N, batch, seed=seed, goals="figure8", dt=DT)
+    kw = solver_kwargs()
+    kw.update(max_sqp_iters=30, pcg_tol=1e-6, max_pcg_iters=400)
+    s = gato_b200.BSQP(batch_size=batch, N=N, dt=DT, plant_type=PLANT, form="fused", **kw)
+    res = s.solve_raw(pr["xu"], DT, pr["xs"], pr["goal"])
+    lam = s.get_lambda()
+    s.close()
+    xu0 = W.perturb(res["XU"], 7, N, pr["rng"]).astype(np.float32)
+    xu0[:, :14] = pr["xs"]
+    return dict(xs=pr["xs"], goal=pr["goal"], xu=xu0, lam=lam)
+
+
+def pcg_flops(pcg_iters, nx=14):
+    """Algorithmic FLOPs of the PCG iterations: per iteration two block-
+    tridiagonal matvecs (2 * N * nx * 3nx multiply-adds each) plus the dot
+    products and vector updates (about 10 flops per padded entry)."""
+    per_it = 2 * (2 * N * nx * 3 * nx) + 10 * (N + 2) * nx
+    return float(np.sum(pcg_iters)) * per_it
+
+
+def knot_flops(nx=14, nu=7):
+    """Algorithmic FLOPs per SQP iteration per problem outside the PCG:
+    Schur complement and preconditioner ((N-1) knots: three Gauss-Jordan
+    inverses of 2n^2(n+1) flops, theta/phi/gamma products, the preconditioner
+    off-diagonal product) and step recovery."""
+    gj = lambda n: 2 * n * n * (n + 1)
+    schur = (N - 1) * (2 * gj(nx) + gj(nu) + 2 * (nx ** 3) * 2 + 2 * nx * nu * nu
+                       + 2 * nx * nx * nu + 4 * nx * nx + 4 * nx ** 3)
+    dz = N * (2 * nx * nx * 2 + 2 * nx * nu * 2 + 2 * nu * nu)
+    return schur + dz
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons during the timed
+    region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def fp32_peak_tflops(torch, dev):
+    """Measured FP32 CUDA-core throughput: cuBLAS SGEMM 8192^3 with TF32
+    disabled, best of 5 (the same kind of measurement as the driver's bf16
+    GEMM peak)."""
+    torch.backends.cuda.matmul.allow_tf32 = False
+    torch.backends.cudnn.allow_tf32 = False
+    n = 8192
+    a = torch.randn(n, n, device=dev, dtype=torch.float32)
+    b = torch.randn(n, n, device=dev, dtype=torch.float32)
+    c = torch.empty(n, n, device=dev, dtype=torch.float32)
+    for _ in range(2):
+        torch.matmul(a, b, out=c)
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+# --------------------------------------------------------------------------
+def cpu_baseline(wl, sample, threads):
+    """The FP64 oracle of the same SQP on `sample` problems of the workload,
+    `threads` host threads; returns (solves/s, seconds)."""
+    from oracle import oracle as O
+    kw = solver_kwargs()
+    P = O.make_params(dt=DT, **kw)
+    S = O.Solver(PLANT, N, sample, P, threads=threads)
+    S.set_lambda(wl["lam"][:sample].astype(np.float64))
+    t0 = time.perf_counter()
+    S.solve(wl["xu"][:sample].astype(np.float64), DT, wl["xs"][:sample].astype(np.float64),
+            wl["goal"][:sample].astype(np.float64))
+    dt = time.perf_counter() - t0
+    return sample / dt, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    sample = args.cpu_sample or max(threads, min(args.batch, 8 * threads))
+    wl = make_cpu_workload(args.batch, sample, threads)
+    for _ in range(args.warmup):
+        cpu_baseline(wl, min(sample, threads), threads)
+    times = []
+    for _ in range(args.steps):
+        v, dt = cpu_baseline(wl, sample, threads)
+        times.append(dt)
+    value = args.steps * sample / float(np.sum(times))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "global_batch": args.batch, "seq_len": N,
+                   "parallelism": f"{threads} host threads"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": f"{sample} problems of the workload per step (FP64 oracle "
+                                   f"port of the reference SQP; the reference's solver has "
+                                   f"no CPU implementation)"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def make_cpu_workload(batch, sample, threads):
+    """The reference arm's copy of the workload: the same seeded problems
+    (first `sample` of the batch) with the warm start made the same way, by
+    a 30-iteration solve from the default warm start (here in the FP64 CPU
+    implementation) and the same seeded perturbation."""
+    from gato_b200 import workloads as W
+    from oracle import oracle as O
+    pr = W.make_problem(PLANT, N, batch, seed=2026, goals="figure8", dt=DT)
+    kw = solver_kwargs()
+    kw.update(max_sqp_iters=30, pcg_tol=1e-6, max_pcg_iters=400)
+    S = O.Solver(PLANT, N, sample, O.make_params(dt=DT, **kw), threads=threads)
+    xu, _ = S.solve(pr["xu"][:sample].astype(np.float64), DT, pr["xs"][:sample],
+                    pr["goal"][:sample])
+    lam = S.get_lambda()
+    full = np.zeros((batch, xu.shape[1]), np.float32)
+    full[:sample] = xu
+    xu0 = W.perturb(full, 7, N, pr["rng"]).astype(np.float32)
+    xu0[:, :14] = pr["xs"]
+    lam_full = np.zeros((batch, lam.shape[1]), np.float32)
+    lam_full[:sample] = lam
+    return dict(xs=pr["xs"], goal=pr["goal"], xu=xu0, lam=lam_full)
+
+
+# --------------------------------------------------------------------------
+def time_device_steps(torch, solver, bufs, wl, steps, warmup, flush, stream):
+    """Per-step CUDA-event times of solver.solve_device (fused graph or plain
+    driver) with warm-start state restored and L2 flushed between steps."""
+    import gato_b200._lib as L
+    d_xu, d_xs, d_goal, d_xu0 = bufs
+    times = []
+    for i in range(warmup + steps):
+        d_xu.copy_(d_xu0)
+        solver.set_lambda(wl["lam"])
+        solver.reset_rho()
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            L.check(L.load().gato_solve(solver._h, stream.cuda_stream, L.vptr(d_xu),
+                                        L.vptr(d_xs), L.vptr(d_goal), None))
+            e1.record(stream)
+        torch.cuda.synchronize()
+        if i >= warmup:
+            times.append(e0.elapsed_time(e1))
+    return np.array(times)
+
+
+def run_ours(args):
+    import torch
+    import gato_b200
+    import gato_b200._lib as L
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+    B = args.batch
+    wl = make_workload(B, seed=2026 + rank)
+    kw = solver_kwargs()
+    fused = gato_b200.BSQP(batch_size=B, N=N, dt=DT, plant_type=PLANT, form="fused",
+                           precision=args.precision, **kw)
+    plain = gato_b200.BSQP(batch_size=B, N=N, dt=DT, plant_type=PLANT, form="plain",
+                           precision=args.precision, **kw)
+    T = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
+    d_xu0, d_xs, d_goal = T(wl["xu"]), T(wl["xs"]), T(wl["goal"])
+    d_xu = d_xu0.clone()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    bufs = (d_xu, d_xs, d_goal, d_xu0)
+
+    # untimed: statistics of one solve (iteration counts for the FLOP count)
+    d_xu.copy_(d_xu0)
+    fused.set_lambda(wl["lam"])
+    fused.reset_rho()
+    st = fused.solve_device(d_xu, d_xs, d_goal, stream=stream.cuda_stream)
+    pcg_total = int(np.sum(st["pcg_iters"]))
+    # per-kernel device times of the same solve (events around each launch)
+    d_xu.copy_(d_xu0)
+    fused.set_lambda(wl["lam"])
+    fused.reset_rho()
+    import ctypes
+    msk = (ctypes.c_double * len(L.KERNELS))()
+    nk = (ctypes.c_int32 * len(L.KERNELS))()
+    L.check(L.load().gato_profile_solve(fused._h, ctypes.c_void_p(stream.cuda_stream),
+                                        L.vptr(d_xu), L.vptr(d_xs), L.vptr(d_goal), msk, nk))
+    kern = {L.KERNELS[i]: {"ms": msk[i], "launches": nk[i]} for i in range(len(L.KERNELS))}
+    total_prof = sum(v["ms"] for v in kern.values())
+
+    peaks = measured_peaks()
+    fp32_peak = fp32_peak_tflops(torch, dev)
+
+    # timed: fused form (headline), clocks sampled during it
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t_fused = time_device_steps(torch, fused, bufs, wl, args.steps, args.warmup, flush, stream)
+    clk = clocks.stop()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    # plain form on the same workload
+    t_plain = time_device_steps(torch, plain, bufs, wl, max(3, args.steps // 2), 1, flush, stream)
+
+    # e2e through the host API (pinned host buffers)
+    h_xu = torch.empty((B, wl["xu"].shape[1]), dtype=torch.float32).pin_memory()
+    h_xs = torch.tensor(wl["xs"]).pin_memory()
+    h_goal = torch.tensor(wl["goal"]).pin_memory()
+    e2e_times = []
+    for i in range(args.warmup + args.steps):
+        h_xu.copy_(torch.from_numpy(wl["xu"]))
+        fused.set_lambda(wl["lam"])
+        fused.reset_rho()
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L.check(L.load().gato_solve_host(fused._h, L.fptr(h_xu), DT, L.fptr(h_xs),
+                                         L.fptr(h_goal), None))
+        t1 = time.perf_counter()
+        if i >= args.warmup:
+            e2e_times.append(t1 - t0)
+    e2e_times = np.array(e2e_times)
+
+    # max over ranks
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms_fused = max_over_ranks(float(np.mean(t_fused)))
+    ms_plain = max_over_ranks(float(np.mean(t_plain)))
+    s_e2e = max_over_ranks(float(np.mean(e2e_times)))
+    p50 = max_over_ranks(float(np.median(t_fused)))
+    p99 = max_over_ranks(float(np.percentile(t_fused, 99)))
+
+    # CPU baseline (rank 0, N=1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        sample = args.cpu_sample or int(min(B, max(threads, 64 * threads)))
+        v, secs = cpu_baseline(wl, sample, threads)
+        cpu = {"value": v, "unit": "solves/s", "cores": threads, "kind": "port",
+               "sample": f"{sample} problems of the workload, one solve, {secs:.1f} s wall "
+                         f"(FP64 oracle port of the reference SQP)"}
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    traj = wl["xu"].shape[1]
+    solves = world * B
+    flops_pcg = pcg_flops(st["pcg_iters"])
+    iters_run = st["ls_num_iters"] + (1 if st["ls_num_iters"] < SQP_ITERS else 0)
+    flops_other = knot_flops() * B * iters_run
+    fi = kern["fused_iter"]
+    fi_ms = fi["ms"] / max(1, fi["launches"])
+    achieved = (flops_pcg + flops_other) / max(1, fi["launches"]) / (fi_ms * 1e-3) / 1e12
+    line = {
+        "metric": METRIC,
+        "value": solves / (ms_fused * 1e-3),
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_fused,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32" if args.precision == "fp32" else "f32+f64-reductions",
+        "data": "synthetic (seeded figure-8 goals, perturbed converged warm start)",
+        "config": {"workload": WORKLOAD + ", form=fused (CUDA graph)",
+                   "global_batch": solves, "seq_len": N, "parallelism": f"replicas x{world}",
+                   "l2": "flushed between steps (256 MB write)"},
+        "p50_latency_ms": p50,
+        "p99_latency_ms": p99,
+        "sqp_iters_per_s": solves * SQP_ITERS / (ms_fused * 1e-3),
+        "plain_form": {"value": solves / (ms_plain * 1e-3), "unit": "solves/s",
+                       "ms_per_step": ms_plain},
+        "fused_vs_plain": ms_plain / ms_fused,
+        "e2e": {"value": solves / s_e2e, "unit": "solves/s",
+                "h2d_bytes_per_step": int(4 * B * (traj + 14 + 6 * N)),
+                "d2h_bytes_per_step": int(4 * B * traj)},
+        "gpu_launches": int(sum(v["launches"] for v in kern.values())) * args.steps,
+        "kernels_ms": {k: round(v["ms"], 4) for k, v in kern.items() if v["launches"]},
+        "pcg_iters_mean": float(np.mean(st["pcg_iters"])),
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                     "kernel": "k_fused_iter", "peak_source": "measured SGEMM (TF32 off)",
+                     "hbm_peak_gbs": peaks.get("hbm_gbs")},
+        "clocks": clk,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,1192 @@
+// C ABI of the solver (include/gato_b200.h): solver object, the plain and
+// fused drivers, CUDA-graph capture, stage entry points and sim_forward.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/gato_b200.h"
+#include "kernels.cuh"
+#include "plant_tables.h"
+
+using namespace gato;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                             \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(GATO_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                                 \
+    } while (0)
+
+#define CKL()                                                                                  \
+    do {                                                                                       \
+        cudaError_t e_ = cudaGetLastError();                                                   \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(GATO_ERR_CUDA, "kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                                   \
+    } while (0)
+
+#define RC(x)                \
+    do {                     \
+        int rc_ = (x);       \
+        if (rc_) return rc_; \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// host model construction in FP64: the same rules as the FP64 oracle,
+// including zeroing transform entries below 1e-6, which reproduces the
+// reference's generated tables.
+constexpr double SNAP = 1e-6;
+
+void rpy_R(const double* rpy, double* R)
+{
+    const double cr = cos(rpy[0]), sr = sin(rpy[0]), cp = cos(rpy[1]), sp = sin(rpy[1]),
+                 cy = cos(rpy[2]), sy = sin(rpy[2]);
+    // Rz(y) Ry(p) Rx(r)
+    R[0] = cy * cp;
+    R[1] = cy * sp * sr - sy * cr;
+    R[2] = cy * sp * cr + sy * sr;
+    R[3] = sy * cp;
+    R[4] = sy * sp * sr + cy * cr;
+    R[5] = sy * sp * cr - cy * sr;
+    R[6] = -sp;
+    R[7] = cp * sr;
+    R[8] = cp * cr;
+}
+
+template <int NQ, typename T>
+void build_dev_model(const gato_model_t& m, DevModel<NQ, T>* out)
+{
+    memset(out, 0, sizeof(*out));
+    for (int i = 0; i < NQ; ++i) {
+        double R[9], E[9], C[9];
+        rpy_R(m.joint_rpy[i], R);
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) E[3 * r + c] = R[3 * c + r];
+        const double* p = m.joint_xyz[i];
+        const double px[9] = {0, -p[2], p[1], p[2], 0, -p[0], -p[1], p[0], 0};
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) {
+                double s = 0;
+                for (int k = 0; k < 3; ++k) s += E[3 * r + k] * px[3 * k + c];
+                C[3 * r + c] = -s;
+            }
+        for (int k = 0; k < 9; ++k) {
+            out->E0[i][k] = (T)(fabs(E[k]) < SNAP ? 0.0 : E[k]);
+            out->C0[i][k] = (T)(fabs(C[k]) < SNAP ? 0.0 : C[k]);
+            out->R0[i][k] = (T)(fabs(R[k]) < SNAP ? 0.0 : R[k]);
+        }
+        for (int k = 0; k < 3; ++k) out->P[i][k] = (T)p[k];
+        double Ib[6] = {0, 0, 0, 0, 0, 0}, h[3] = {0, 0, 0}, mass = 0;
+        for (int bdy = 0; bdy < 2; ++bdy) {
+            const double* bd = m.link_inertial[i][bdy];
+            const double mm = bd[0];
+            if (mm == 0.0) continue;
+            const double cx = bd[1], cy = bd[2], cz = bd[3];
+            const double c2 = cx * cx + cy * cy + cz * cz;
+            Ib[0] += bd[4] + mm * (c2 - cx * cx);
+            Ib[1] += bd[5] - mm * cx * cy;
+            Ib[2] += bd[6] - mm * cx * cz;
+            Ib[3] += bd[7] + mm * (c2 - cy * cy);
+            Ib[4] += bd[8] - mm * cy * cz;
+            Ib[5] += bd[9] + mm * (c2 - cz * cz);
+            h[0] += mm * cx;
+            h[1] += mm * cy;
+            h[2] += mm * cz;
+            mass += mm;
+        }
+        for (int k = 0; k < 6; ++k) out->Ibar[i][k] = (T)Ib[k];
+        for (int k = 0; k < 3; ++k) out->h[i][k] = (T)h[k];
+        out->mass[i] = (T)mass;
+        const double mg = m.limit_margin;
+        out->qlo[i] = (T)(-m.q_limit[i] - mg);
+        out->qhi[i] = (T)(m.q_limit[i] + mg);
+        out->vlo[i] = (T)(-m.qd_limit[i] - mg);
+        out->vhi[i] = (T)(m.qd_limit[i] + mg);
+        out->ulo[i] = (T)(-m.u_limit[i] - mg);
+        out->uhi[i] = (T)(m.u_limit[i] + mg);
+    }
+    out->gravity = (T)m.gravity;
+    out->barrier_style = m.barrier_style;
+}
+
+template <class K>
+int set_smem(K kernel, size_t bytes)
+{
+    if (bytes > 48 * 1024)
+        CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return GATO_OK;
+}
+
+// (joints, scalar, reduction scalar) of a solver instance
+template <int NQ_, typename T_, typename Acc_>
+struct Tag {
+    static constexpr int NQ = NQ_;
+    using T = T_;
+    using Acc = Acc_;
+};
+
+}  // namespace
+
+// ===========================================================================
+struct gato_solver {
+    int nq = 0, N = 0, B = 0, form = 0, precision = 0, device = 0;
+    size_t esz = 4;  // bytes of the solver scalar
+    gato_model_t model;
+    gato_params_t params;
+    double dt = 0.01;
+    int adapt_rho = 1;
+    int use_fext = 0;
+    int max_smem = 0;
+    // device memory, scalar-typed buffers as raw pointers
+    void *xu = nullptr, *xs = nullptr, *goal = nullptr, *fext = nullptr;
+    void *Q = nullptr, *R = nullptr, *q = nullptr, *r = nullptr, *A = nullptr, *Bm = nullptr,
+         *c = nullptr, *Qi = nullptr, *Ri = nullptr;
+    void *S = nullptr, *P = nullptr, *gamma = nullptr, *lambda = nullptr, *dz = nullptr;
+    void *rho = nullptr, *drho = nullptr, *mu = nullptr, *tol = nullptr, *drho_init_d = nullptr;
+    void *sim_x = nullptr, *sim_u = nullptr, *sim_out = nullptr;
+    double *merit_terms = nullptr, *merit_init = nullptr, *merit_init0 = nullptr,
+           *merit_final = nullptr;
+    int *pcg_iters = nullptr, *conv = nullptr, *sqp_iters = nullptr, *done = nullptr,
+        *ls_count = nullptr, *h_pcg = nullptr;
+    float *h_ls_min = nullptr, *h_ls_step = nullptr;
+    // host
+    std::vector<double> rho_init, drho_init;
+    int* pin_i = nullptr;  // pinned host ints (B)
+    cudaStream_t own_stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // fused-form graph cache
+    cudaGraphExec_t gexec = nullptr;
+    const void* gkey[4] = {nullptr, nullptr, nullptr, nullptr};
+    int gver = -1;
+    int version = 0;  // bumped when a value baked into kernel arguments changes
+    std::vector<void*> allocs;
+    alignas(16) unsigned char dev_model[sizeof(DevModel<8, double>)];
+    // optional per-launch event timing (never during graph capture)
+    struct ProfEntry {
+        int id;
+        cudaEvent_t a, b;
+    };
+    std::vector<ProfEntry>* prof = nullptr;
+
+    int alloc_bytes(void** p, size_t bytes)
+    {
+        void* v = nullptr;
+        bytes = std::max<size_t>(bytes, 16);
+        CK(cudaMalloc(&v, bytes));
+        CK(cudaMemset(v, 0, bytes));
+        allocs.push_back(v);
+        *p = v;
+        return GATO_OK;
+    }
+    template <class U>
+    int alloc(U** p, size_t count)
+    {
+        return alloc_bytes((void**)p, count * sizeof(U));
+    }
+    int alloc_t(void** p, size_t count) { return alloc_bytes(p, count * esz); }
+    // host scalar array -> device scalar array
+    int upload(void* dst, const double* src, size_t n)
+    {
+        if (esz == sizeof(double)) {
+            CK(cudaMemcpy(dst, src, n * sizeof(double), cudaMemcpyHostToDevice));
+        } else {
+            std::vector<float> t(src, src + n);
+            CK(cudaMemcpy(dst, t.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+        }
+        return GATO_OK;
+    }
+};
+
+namespace {
+
+template <class F>
+int dispatch(gato_solver* s, F&& f)
+{
+    if (s->nq == 7) {
+        if (s->precision == GATO_PREC_FP64) return f(Tag<7, double, double>());
+        if (s->precision == GATO_PREC_MIXED) return f(Tag<7, float, double>());
+        return f(Tag<7, float, float>());
+    }
+    if (s->precision == GATO_PREC_FP64) return f(Tag<6, double, double>());
+    if (s->precision == GATO_PREC_MIXED) return f(Tag<6, float, double>());
+    return f(Tag<6, float, float>());
+}
+
+template <class Tg>
+Batch<Tg::NQ, typename Tg::T> make_batch(gato_solver* s, void* xu, const void* xs, const void* goal)
+{
+    using T = typename Tg::T;
+    Batch<Tg::NQ, T> b;
+    b.B = s->B;
+    b.N = s->N;
+    b.solve_ratio = (float)s->params.solve_ratio;
+    b.max_pcg_iters = s->params.max_pcg_iters;
+    b.adapt_rho = s->adapt_rho;
+    b.cp.dt = (T)s->dt;
+    b.cp.q_cost = (T)s->params.q_cost;
+    b.cp.qd_cost = (T)s->params.qd_cost;
+    b.cp.u_cost = (T)s->params.u_cost;
+    b.cp.N_cost = (T)s->params.N_cost;
+    b.cp.q_lim_cost = (T)s->params.q_lim_cost;
+    b.cp.vel_lim_cost = (T)s->params.vel_lim_cost;
+    b.cp.ctrl_lim_cost = (T)s->params.ctrl_lim_cost;
+    b.xu = (T*)xu;
+    b.xs = (const T*)xs;
+    b.goal = (const T*)goal;
+    b.fext = (const T*)s->fext;
+    b.use_fext = s->use_fext;
+    b.Q = (T*)s->Q;
+    b.R = (T*)s->R;
+    b.q = (T*)s->q;
+    b.r = (T*)s->r;
+    b.A = (T*)s->A;
+    b.Bm = (T*)s->Bm;
+    b.c = (T*)s->c;
+    b.Qi = (T*)s->Qi;
+    b.Ri = (T*)s->Ri;
+    b.S = (T*)s->S;
+    b.P = (T*)s->P;
+    b.gamma = (T*)s->gamma;
+    b.lambda = (T*)s->lambda;
+    b.dz = (T*)s->dz;
+    b.rho = (T*)s->rho;
+    b.drho = (T*)s->drho;
+    b.mu = (T*)s->mu;
+    b.tol = (T*)s->tol;
+    b.merit_terms = s->merit_terms;
+    b.merit_init = s->merit_init;
+    b.merit_init0 = s->merit_init0;
+    b.merit_final = s->merit_final;
+    b.pcg_iters = s->pcg_iters;
+    b.conv = s->conv;
+    b.sqp_iters = s->sqp_iters;
+    b.done = s->done;
+    b.ls_count = s->ls_count;
+    b.h_pcg = s->h_pcg;
+    b.h_ls_min = s->h_ls_min;
+    b.h_ls_step = s->h_ls_step;
+    return b;
+}
+
+constexpr int WPB = 4;  // warps per block of the per-knot kernels
+constexpr int PCG_THREADS = 256;
+constexpr int FUSED_THREADS = 256;
+constexpr int LS_THREADS = 128;
+
+inline int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+// Brackets one launch with events when profiling is on.
+struct ProfScope {
+    gato_solver* s;
+    cudaStream_t st;
+    int id;
+    cudaEvent_t a = nullptr, b = nullptr;
+    ProfScope(gato_solver* s_, cudaStream_t st_, int id_) : s(s_), st(st_), id(id_)
+    {
+        if (!s->prof) return;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, st);
+    }
+    ~ProfScope()
+    {
+        if (!s->prof) return;
+        cudaEventRecord(b, st);
+        s->prof->push_back({id, a, b});
+    }
+};
+
+template <class Tg>
+const DevModel<Tg::NQ, typename Tg::T>& dmodel(gato_solver* s)
+{
+    return *reinterpret_cast<const DevModel<Tg::NQ, typename Tg::T>*>(s->dev_model);
+}
+
+template <class Tg>
+bool pcg_stage_fits(gato_solver* s)
+{
+    return pcg_smem_bytes<Tg::NQ, typename Tg::T>(s->N, true) <= (size_t)s->max_smem;
+}
+
+template <class Tg>
+bool fused_stage_fits(gato_solver* s)
+{
+    FusedLayout<Tg::NQ, typename Tg::T> lay{s->N, FUSED_THREADS / WARP, true};
+    return lay.bytes() <= (size_t)s->max_smem;
+}
+
+// --- stage launchers ---------------------------------------------------------
+template <class Tg>
+int launch_merit(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt,
+                 int nalpha, int use_dz, int skip)
+{
+    constexpr int NQ = Tg::NQ;
+    using T = typename Tg::T;
+    ProfScope ps_(s, st, GATO_KERNEL_MERIT);
+    const size_t sm = WPB * MeritSmem<NQ>::SIZE * sizeof(T);
+    dim3 grid(cdiv(s->N * nalpha, WPB), s->B);
+    k_merit<NQ, T><<<grid, WPB * WARP, sm, st>>>(bt, dmodel<Tg>(s), nalpha, use_dz, skip);
+    CKL();
+    return GATO_OK;
+}
+
+template <class Tg>
+int launch_merit_sum(gato_solver* s, cudaStream_t st, double* out, double* out2)
+{
+    ProfScope ps_(s, st, GATO_KERNEL_MERIT_SUM);
+    k_merit_sum<typename Tg::Acc><<<cdiv(s->B, 128), 128, 0, st>>>(s->B, s->N, s->merit_terms,
+                                                                    out, out2);
+    CKL();
+    return GATO_OK;
+}
+
+template <class Tg>
+int launch_kkt(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt)
+{
+    constexpr int NQ = Tg::NQ;
+    using T = typename Tg::T;
+    ProfScope ps_(s, st, GATO_KERNEL_KKT);
+    const size_t sm = WPB * KktSmem<NQ>::SIZE * sizeof(T);
+    k_kkt<NQ, T><<<dim3(cdiv(s->N - 1, WPB), s->B), WPB * WARP, sm, st>>>(bt, dmodel<Tg>(s));
+    CKL();
+    return GATO_OK;
+}
+
+template <class Tg>
+int launch_schur(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt)
+{
+    constexpr int NQ = Tg::NQ;
+    using T = typename Tg::T;
+    ProfScope ps_(s, st, GATO_KERNEL_SCHUR);
+    k_schur_inv<NQ, T><<<dim3(cdiv(s->N, WPB), s->B), WPB * WARP, 0, st>>>(bt);
+    CKL();
+    const size_t sm = WPB * SchurSmem<NQ>::SIZE * sizeof(T);
+    k_schur<NQ, T><<<dim3(cdiv(s->N, WPB), s->B), WPB * WARP, sm, st>>>(bt);
+    CKL();
+    const size_t sm2 = WPB * 4 * (2 * NQ) * (2 * NQ) * sizeof(T);
+    k_schur_off<NQ, T><<<dim3(cdiv(s->N - 1, WPB), s->B), WPB * WARP, sm2, st>>>(bt);
+    CKL();
+    return GATO_OK;
+}
+
+template <class Tg>
+int launch_pcg(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt, int row)
+{
+    constexpr int NQ = Tg::NQ;
+    using T = typename Tg::T;
+    ProfScope ps_(s, st, GATO_KERNEL_PCG);
+    const bool stage = pcg_stage_fits<Tg>(s);
+    const size_t sm = pcg_smem_bytes<NQ, T>(s->N, stage);
+    k_pcg<NQ, T, typename Tg::Acc><<<s->B, PCG_THREADS, sm, st>>>(bt, stage, row);
+    CKL();
+    return GATO_OK;
+}
+
+template <class Tg>
+int launch_dz(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt)
+{
+    constexpr int NQ = Tg::NQ;
+    using T = typename Tg::T;
+    ProfScope ps_(s, st, GATO_KERNEL_DZ);
+    const size_t sm = WPB * 3 * (2 * NQ) * sizeof(T);
+    k_dz<NQ, T><<<dim3(cdiv(s->N, WPB), s->B), WPB * WARP, sm, st>>>(bt);
+    CKL();
+    return GATO_OK;
+}
+
+template <class Tg>
+int launch_ls(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt, int row,
+              int skip)
+{
+    ProfScope ps_(s, st, GATO_KERNEL_LINE_SEARCH);
+    k_line_search<Tg::NQ, typename Tg::T, typename Tg::Acc><<<s->B, LS_THREADS, 0, st>>>(bt, row,
+                                                                                      skip);
+    CKL();
+    return GATO_OK;
+}
+
+template <class Tg>
+int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt,
+                      int row)
+{
+    constexpr int NQ = Tg::NQ;
+    using T = typename Tg::T;
+    ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
+    const bool stage = fused_stage_fits<Tg>(s);
+    FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, stage};
+    k_fused_iter<NQ, T, typename Tg::Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(
+        bt, dmodel<Tg>(s), stage, row);
+    CKL();
+    return GATO_OK;
+}
+
+template <class Tg>
+int launch_check(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt)
+{
+    ProfScope ps_(s, st, GATO_KERNEL_CHECK);
+    k_check<Tg::NQ, typename Tg::T><<<1, 1024, 0, st>>>(bt);
+    CKL();
+    return GATO_OK;
+}
+
+template <class Tg>
+int configure_kernels(gato_solver* s)
+{
+    constexpr int NQ = Tg::NQ;
+    using T = typename Tg::T;
+    using Acc = typename Tg::Acc;
+    RC(set_smem(k_pcg<NQ, T, Acc>, pcg_smem_bytes<NQ, T>(s->N, pcg_stage_fits<Tg>(s))));
+    FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, fused_stage_fits<Tg>(s)};
+    if (lay.bytes() > (size_t)s->max_smem)
+        return fail(GATO_ERR_UNSUPPORTED, "N=%d needs %zu bytes of shared memory", s->N,
+                    lay.bytes());
+    RC(set_smem(k_fused_iter<NQ, T, Acc>, lay.bytes()));
+    return GATO_OK;
+}
+
+// --- solve drivers -------------------------------------------------------------
+// Reference driver shape (gato/bsqp/bsqp.cuh:103-197): stage kernels and a
+// host convergence check after every PCG.
+template <class Tg>
+int solve_plain(gato_solver* s, cudaStream_t st, void* xu, const void* xs, const void* goal,
+                int* host_sqp, int* host_conv, int* ls_rows)
+{
+    const int B = s->B, N = s->N;
+    const Dims<Tg::NQ> d{N};
+    auto bt = make_batch<Tg>(s, xu, xs, goal);
+    CK(cudaMemsetAsync(s->dz, 0, s->esz * (size_t)B * d.traj(), st));
+    CK(cudaMemsetAsync(s->conv, 0, sizeof(int) * B, st));
+    RC(launch_merit<Tg>(s, st, bt, 1, 0, 0));
+    RC(launch_merit_sum<Tg>(s, st, s->merit_init, s->merit_init0));
+    std::fill(host_sqp, host_sqp + B, 0);
+    std::fill(host_conv, host_conv + B, 0);
+    int rows = 0;
+    for (int it = 0; it < s->params.max_sqp_iters; ++it) {
+        RC(launch_kkt<Tg>(s, st, bt));
+        RC(launch_schur<Tg>(s, st, bt));
+        RC(launch_pcg<Tg>(s, st, bt, it));
+        RC(launch_dz<Tg>(s, st, bt));
+        CK(cudaMemcpyAsync(s->pin_i, s->pcg_iters, sizeof(int) * B, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        int solved = 0;
+        for (int b = 0; b < B; ++b) {
+            if (s->pin_i[b] == 0) {
+                host_conv[b] = 1;
+                host_sqp[b] += 1;
+            }
+            if (host_conv[b]) solved++;
+            else host_sqp[b] += 1;
+        }
+        if ((float)solved >= (float)B * (float)s->params.solve_ratio) break;
+        memcpy(s->pin_i, host_conv, sizeof(int) * B);
+        CK(cudaMemcpyAsync(s->conv, s->pin_i, sizeof(int) * B, cudaMemcpyHostToDevice, st));
+        RC(launch_merit<Tg>(s, st, bt, NUM_ALPHAS, 1, 0));
+        RC(launch_ls<Tg>(s, st, bt, it, 0));
+        rows++;
+    }
+    RC(launch_merit<Tg>(s, st, bt, 1, 0, 0));
+    RC(launch_merit_sum<Tg>(s, st, s->merit_final, nullptr));
+    CK(cudaMemcpyAsync(s->drho, s->drho_init_d, s->esz * B, cudaMemcpyDeviceToDevice, st));
+    *ls_rows = rows;
+    return GATO_OK;
+}
+
+// Device-side control flow: enqueues the whole solve (no host round trip).
+template <class Tg>
+int enqueue_fused(gato_solver* s, cudaStream_t st, void* xu, const void* xs, const void* goal)
+{
+    const int B = s->B, N = s->N;
+    const Dims<Tg::NQ> d{N};
+    auto bt = make_batch<Tg>(s, xu, xs, goal);
+    CK(cudaMemsetAsync(s->dz, 0, s->esz * (size_t)B * d.traj(), st));
+    CK(cudaMemsetAsync(s->conv, 0, sizeof(int) * B, st));
+    CK(cudaMemsetAsync(s->sqp_iters, 0, sizeof(int) * B, st));
+    CK(cudaMemsetAsync(s->done, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(s->ls_count, 0, sizeof(int), st));
+    RC(launch_merit<Tg>(s, st, bt, 1, 0, 0));
+    RC(launch_merit_sum<Tg>(s, st, s->merit_init, s->merit_init0));
+    for (int it = 0; it < s->params.max_sqp_iters; ++it) {
+        RC(launch_fused_iter<Tg>(s, st, bt, it));
+        RC(launch_check<Tg>(s, st, bt));
+        RC(launch_merit<Tg>(s, st, bt, NUM_ALPHAS, 1, 1));
+        RC(launch_ls<Tg>(s, st, bt, it, 1));
+    }
+    RC(launch_merit<Tg>(s, st, bt, 1, 0, 0));
+    RC(launch_merit_sum<Tg>(s, st, s->merit_final, nullptr));
+    CK(cudaMemcpyAsync(s->drho, s->drho_init_d, s->esz * B, cudaMemcpyDeviceToDevice, st));
+    return GATO_OK;
+}
+
+template <class Tg>
+int solve_fused(gato_solver* s, cudaStream_t st, void* xu, const void* xs, const void* goal)
+{
+    const bool stale = s->gexec == nullptr || s->gkey[0] != xu || s->gkey[1] != xs ||
+                       s->gkey[2] != goal || s->gkey[3] != (const void*)st || s->gver != s->version;
+    if (stale) {
+        if (s->gexec) {
+            cudaGraphExecDestroy(s->gexec);
+            s->gexec = nullptr;
+        }
+        cudaStream_t cap;
+        CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        CK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_fused<Tg>(s, cap, xu, xs, goal);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(cap, &graph);
+        cudaStreamDestroy(cap);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (e != cudaSuccess) return fail(GATO_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&s->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return fail(GATO_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        s->gkey[0] = xu;
+        s->gkey[1] = xs;
+        s->gkey[2] = goal;
+        s->gkey[3] = (const void*)st;
+        s->gver = s->version;
+    }
+    CK(cudaGraphLaunch(s->gexec, st));
+    return GATO_OK;
+}
+
+int read_stats(gato_solver* s, const int* hsqp, const int* hconv, int rows, gato_stats_t* stats)
+{
+    const int B = s->B;
+    const int iters = std::max(1, s->params.max_sqp_iters);
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    stats->sqp_time_us = 1000.0 * ms;
+    stats->ls_num_iters = rows;
+    if (stats->sqp_iters) memcpy(stats->sqp_iters, hsqp, sizeof(int) * B);
+    if (stats->kkt_converged) memcpy(stats->kkt_converged, hconv, sizeof(int) * B);
+    std::vector<double> tmp(B);
+    if (stats->final_merit) {
+        CK(cudaMemcpy(tmp.data(), s->merit_final, sizeof(double) * B, cudaMemcpyDeviceToHost));
+        for (int b = 0; b < B; ++b) stats->final_merit[b] = (float)tmp[b];
+    }
+    if (stats->initial_merit) {
+        CK(cudaMemcpy(tmp.data(), s->merit_init0, sizeof(double) * B, cudaMemcpyDeviceToHost));
+        for (int b = 0; b < B; ++b) stats->initial_merit[b] = (float)tmp[b];
+    }
+    if (stats->pcg_iters)
+        CK(cudaMemcpy(stats->pcg_iters, s->h_pcg, sizeof(int) * (size_t)iters * B,
+                      cudaMemcpyDeviceToHost));
+    if (stats->ls_min_merit)
+        CK(cudaMemcpy(stats->ls_min_merit, s->h_ls_min, sizeof(float) * (size_t)iters * B,
+                      cudaMemcpyDeviceToHost));
+    if (stats->ls_step_size)
+        CK(cudaMemcpy(stats->ls_step_size, s->h_ls_step, sizeof(float) * (size_t)iters * B,
+                      cudaMemcpyDeviceToHost));
+    return GATO_OK;
+}
+
+template <class Tg>
+int do_solve(gato_solver* s, cudaStream_t st, void* xu, const void* xs, const void* goal,
+             gato_stats_t* stats)
+{
+    const int B = s->B;
+    std::vector<int> hsqp(B), hconv(B);
+    int rows = 0;
+    CK(cudaEventRecord(s->ev0, st));
+    if (s->form == GATO_FORM_PLAIN)
+        RC(solve_plain<Tg>(s, st, xu, xs, goal, hsqp.data(), hconv.data(), &rows));
+    else
+        RC(solve_fused<Tg>(s, st, xu, xs, goal));
+    CK(cudaEventRecord(s->ev1, st));
+    if (!stats) return GATO_OK;
+    CK(cudaStreamSynchronize(st));
+    if (s->form != GATO_FORM_PLAIN) {
+        CK(cudaMemcpy(&rows, s->ls_count, sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hsqp.data(), s->sqp_iters, sizeof(int) * B, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hconv.data(), s->conv, sizeof(int) * B, cudaMemcpyDeviceToHost));
+    }
+    return read_stats(s, hsqp.data(), hconv.data(), rows, stats);
+}
+
+// sim_forward: one warp per problem (simForwardBatchedKernel,
+// gato/bsqp/kernels/sim.cuh:14-49).
+template <int NQ, typename T>
+__global__ void k_sim_forward(DevModel<NQ, T> M, int B, T dt, const T* xk, const T* uk,
+                              const T* fext, int use_fext, T* out)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
+    const int b = blockIdx.x * (blockDim.x / WARP) + warp_id();
+    if (b >= B) return;
+    T* s = smem + warp_id() * DynSmem<NQ>::SIZE;
+    const T* q = xk;
+    const T* qd = xk + NQ;
+    dyn_load_transforms<NQ, T>(M, q, s);
+    __syncwarp();
+    T mc[NQ];
+    dyn_forward<NQ, T>(M, s, q, qd, uk, use_fext ? fext + 6 * b : nullptr, false, mc);
+    const int l = lane_id();
+    if (l < 2 * NQ) {
+        T v;
+        if (l < NQ)
+            v = q[l] + dt * qd[l] + T(0.5) * s[DynSmem<NQ>::QDD + l] * dt * dt;
+        else
+            v = qd[l - NQ] + dt * s[DynSmem<NQ>::QDD + l - NQ];
+        out[(size_t)b * 2 * NQ + l] = v;
+    }
+}
+
+cudaStream_t as_stream(void* st) { return (cudaStream_t)st; }
+
+int check_handle(const gato_solver* s)
+{
+    if (!s) return fail(GATO_ERR_ARG, "null solver handle");
+    return GATO_OK;
+}
+
+int bind_device(const gato_solver* s)
+{
+    int cur = -1;
+    CK(cudaGetDevice(&cur));
+    if (cur != s->device) CK(cudaSetDevice(s->device));
+    return GATO_OK;
+}
+
+int check_single(const gato_solver* s)
+{
+    if (s->precision == GATO_PREC_FP64)
+        return fail(GATO_ERR_ARG, "FP64 solver: use the _f64 entry points");
+    return GATO_OK;
+}
+
+int check_double(const gato_solver* s)
+{
+    if (s->precision != GATO_PREC_FP64)
+        return fail(GATO_ERR_ARG, "_f64 entry point on a single-precision solver");
+    return GATO_OK;
+}
+
+int solve_host_any(gato_solver* s, void* h_xu, double dt, const void* h_xs, const void* h_goal,
+                   gato_stats_t* stats)
+{
+    RC(bind_device(s));
+    if (dt != s->dt) {
+        s->dt = dt;
+        s->version++;
+    }
+    const int nx = 2 * s->nq, nu = s->nq;
+    const size_t traj = (size_t)(nx + nu) * s->N - nu;
+    cudaStream_t st = s->own_stream;
+    CK(cudaMemcpyAsync(s->xu, h_xu, s->esz * traj * s->B, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->xs, h_xs, s->esz * nx * s->B, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->goal, h_goal, s->esz * 6 * s->N * s->B, cudaMemcpyHostToDevice, st));
+    RC(dispatch(s, [&](auto tg) {
+        return do_solve<decltype(tg)>(s, st, s->xu, s->xs, s->goal, stats);
+    }));
+    CK(cudaMemcpyAsync(h_xu, s->xu, s->esz * traj * s->B, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return GATO_OK;
+}
+
+int set_batch(gato_solver_t* s, void* d, const float* h, std::vector<double>* dflt, int as_default)
+{
+    RC(check_handle(s));
+    if (!h) return fail(GATO_ERR_ARG, "null host array");
+    RC(bind_device(s));
+    std::vector<double> v(h, h + s->B);
+    RC(s->upload(d, v.data(), s->B));
+    if (dflt && as_default) *dflt = v;
+    return GATO_OK;
+}
+
+int lambda_count(const gato_solver* s) { return s->B * (s->N + 2) * 2 * s->nq; }
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char* gato_last_error(void) { return g_err.c_str(); }
+
+const char* gato_version(void) { return "gato_b200 0.2 (sm_100a)"; }
+
+int gato_builtin_model(int plant, gato_model_t* out)
+{
+    if (!out) return fail(GATO_ERR_ARG, "null model pointer");
+    if (gato_plant_fill(plant, out) != 0) return fail(GATO_ERR_ARG, "unknown plant %d", plant);
+    return GATO_OK;
+}
+
+int gato_create(const gato_model_t* model, int N, int batch, const gato_params_t* params,
+                int form, int precision, gato_solver_t** out)
+{
+    if (!out) return fail(GATO_ERR_ARG, "null output pointer");
+    *out = nullptr;
+    if (!model || !params) return fail(GATO_ERR_ARG, "null model or params");
+    if (model->nq != 6 && model->nq != 7)
+        return fail(GATO_ERR_UNSUPPORTED, "nq=%d: built for 6 or 7 joints", model->nq);
+    if (N < 2 || N > 256) return fail(GATO_ERR_ARG, "N=%d out of range [2, 256]", N);
+    if (batch < 1 || batch > 65535) return fail(GATO_ERR_ARG, "batch=%d out of range", batch);
+    if (form != GATO_FORM_PLAIN && form != GATO_FORM_FUSED)
+        return fail(GATO_ERR_ARG, "unknown form %d", form);
+    if (precision != GATO_PREC_FP32 && precision != GATO_PREC_MIXED &&
+        precision != GATO_PREC_FP64)
+        return fail(GATO_ERR_ARG, "unknown precision %d", precision);
+    if (params->max_sqp_iters < 0 || params->max_pcg_iters < 0)
+        return fail(GATO_ERR_ARG, "negative iteration limits");
+    if (!(params->dt > 0.0)) return fail(GATO_ERR_ARG, "dt must be positive");
+    std::unique_ptr<gato_solver> s(new gato_solver);
+    gato_solver* p = s.get();
+    p->nq = model->nq;
+    p->N = N;
+    p->B = batch;
+    p->form = form;
+    p->precision = precision;
+    p->esz = precision == GATO_PREC_FP64 ? sizeof(double) : sizeof(float);
+    p->model = *model;
+    p->params = *params;
+    p->dt = params->dt;
+    CK(cudaGetDevice(&p->device));
+    CK(cudaDeviceGetAttribute(&p->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device));
+    dispatch(p, [&](auto tg) {
+        using Tg = decltype(tg);
+        build_dev_model<Tg::NQ, typename Tg::T>(*model,
+                                                (DevModel<Tg::NQ, typename Tg::T>*)p->dev_model);
+        return 0;
+    });
+    const int nx = 2 * p->nq, nu = p->nq;
+    const size_t B = batch;
+    const size_t traj = (size_t)(nx + nu) * N - nu, vecp = (size_t)(N + 2) * nx,
+                 b3d = (size_t)3 * nx * nx * N;
+    const int iters = std::max(1, params->max_sqp_iters);
+    RC(p->alloc_t(&p->xu, B * traj));
+    RC(p->alloc_t(&p->xs, B * nx));
+    RC(p->alloc_t(&p->goal, B * 6 * N));
+    RC(p->alloc_t(&p->fext, B * 6));
+    RC(p->alloc_t(&p->Q, B * N * nx * nx));
+    RC(p->alloc_t(&p->R, B * N * nu * nu));
+    RC(p->alloc_t(&p->q, B * N * nx));
+    RC(p->alloc_t(&p->r, B * N * nu));
+    RC(p->alloc_t(&p->A, B * N * nx * nx));
+    RC(p->alloc_t(&p->Bm, B * N * nx * nu));
+    RC(p->alloc_t(&p->c, B * N * nx));
+    RC(p->alloc_t(&p->Qi, B * N * nx * nx));
+    RC(p->alloc_t(&p->Ri, B * N * nu * nu));
+    RC(p->alloc_t(&p->S, B * b3d));
+    RC(p->alloc_t(&p->P, B * b3d));
+    RC(p->alloc_t(&p->gamma, B * vecp));
+    RC(p->alloc_t(&p->lambda, B * vecp));
+    RC(p->alloc_t(&p->dz, B * traj));
+    RC(p->alloc_t(&p->rho, B));
+    RC(p->alloc_t(&p->drho, B));
+    RC(p->alloc_t(&p->mu, B));
+    RC(p->alloc_t(&p->tol, B));
+    RC(p->alloc_t(&p->drho_init_d, B));
+    RC(p->alloc_t(&p->sim_x, nx));
+    RC(p->alloc_t(&p->sim_u, nu));
+    RC(p->alloc_t(&p->sim_out, B * nx));
+    RC(p->alloc(&p->merit_terms, B * NUM_ALPHAS * N));
+    RC(p->alloc(&p->merit_init, B));
+    RC(p->alloc(&p->merit_init0, B));
+    RC(p->alloc(&p->merit_final, B));
+    RC(p->alloc(&p->pcg_iters, B));
+    RC(p->alloc(&p->conv, B));
+    RC(p->alloc(&p->sqp_iters, B));
+    RC(p->alloc(&p->done, 1));
+    RC(p->alloc(&p->ls_count, 1));
+    RC(p->alloc(&p->h_pcg, (size_t)iters * B));
+    RC(p->alloc(&p->h_ls_min, (size_t)iters * B));
+    RC(p->alloc(&p->h_ls_step, (size_t)iters * B));
+    CK(cudaMallocHost(&p->pin_i, sizeof(int) * B));
+    CK(cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&p->ev0));
+    CK(cudaEventCreate(&p->ev1));
+    // BSQP constructor defaults (bsqp.cuh:46-58): drho = 1, rho/mu/tol from
+    // the parameters (float in the reference's FP32 build)
+    const bool f64 = precision == GATO_PREC_FP64;
+    auto as_t = [&](double v) { return f64 ? v : (double)(float)v; };
+    p->rho_init.assign(B, as_t(params->rho));
+    p->drho_init.assign(B, 1.0);
+    std::vector<double> mu(B, as_t(params->mu)), tol(B, as_t(params->pcg_tol));
+    RC(p->upload(p->rho, p->rho_init.data(), B));
+    RC(p->upload(p->drho, p->drho_init.data(), B));
+    RC(p->upload(p->drho_init_d, p->drho_init.data(), B));
+    RC(p->upload(p->mu, mu.data(), B));
+    RC(p->upload(p->tol, tol.data(), B));
+    RC(dispatch(p, [&](auto tg) { return configure_kernels<decltype(tg)>(p); }));
+    CK(cudaDeviceSynchronize());
+    *out = s.release();
+    return GATO_OK;
+}
+
+void gato_destroy(gato_solver_t* s)
+{
+    if (!s) return;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    cudaSetDevice(s->device);
+    if (s->gexec) cudaGraphExecDestroy(s->gexec);
+    for (void* v : s->allocs) cudaFree(v);
+    if (s->pin_i) cudaFreeHost(s->pin_i);
+    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (cur >= 0) cudaSetDevice(cur);
+    delete s;
+}
+
+int gato_sizes(const gato_solver_t* s, int* nx, int* nu, int* traj_size, int* goal_size,
+               int* lambda_size)
+{
+    RC(check_handle(s));
+    const int x = 2 * s->nq, u = s->nq;
+    if (nx) *nx = x;
+    if (nu) *nu = u;
+    if (traj_size) *traj_size = (x + u) * s->N - u;
+    if (goal_size) *goal_size = 6 * s->N;
+    if (lambda_size) *lambda_size = (s->N + 2) * x;
+    return GATO_OK;
+}
+
+int gato_solve(gato_solver_t* s, void* stream, float* d_xu, const float* d_xs,
+               const float* d_goal, gato_stats_t* stats)
+{
+    RC(check_handle(s));
+    RC(check_single(s));
+    if (!d_xu || !d_xs || !d_goal) return fail(GATO_ERR_ARG, "null device buffer");
+    RC(bind_device(s));
+    return dispatch(s, [&](auto tg) {
+        return do_solve<decltype(tg)>(s, as_stream(stream), d_xu, d_xs, d_goal, stats);
+    });
+}
+
+int gato_solve_f64(gato_solver_t* s, void* stream, double* d_xu, const double* d_xs,
+                   const double* d_goal, gato_stats_t* stats)
+{
+    RC(check_handle(s));
+    RC(check_double(s));
+    if (!d_xu || !d_xs || !d_goal) return fail(GATO_ERR_ARG, "null device buffer");
+    RC(bind_device(s));
+    return dispatch(s, [&](auto tg) {
+        return do_solve<decltype(tg)>(s, as_stream(stream), d_xu, d_xs, d_goal, stats);
+    });
+}
+
+int gato_solve_host(gato_solver_t* s, float* h_xu, float dt, const float* h_xs,
+                    const float* h_goal, gato_stats_t* stats)
+{
+    RC(check_handle(s));
+    RC(check_single(s));
+    if (!h_xu || !h_xs || !h_goal) return fail(GATO_ERR_ARG, "null host buffer");
+    if (!(dt > 0.0f)) return fail(GATO_ERR_ARG, "dt must be positive");
+    return solve_host_any(s, h_xu, (double)dt, h_xs, h_goal, stats);
+}
+
+int gato_solve_host_f64(gato_solver_t* s, double* h_xu, double dt, const double* h_xs,
+                        const double* h_goal, gato_stats_t* stats)
+{
+    RC(check_handle(s));
+    RC(check_double(s));
+    if (!h_xu || !h_xs || !h_goal) return fail(GATO_ERR_ARG, "null host buffer");
+    if (!(dt > 0.0)) return fail(GATO_ERR_ARG, "dt must be positive");
+    return solve_host_any(s, h_xu, dt, h_xs, h_goal, stats);
+}
+
+int gato_profile_solve(gato_solver_t* s, void* stream, float* d_xu, const float* d_xs,
+                       const float* d_goal, double* ms_by_kernel, int32_t* launches_by_kernel)
+{
+    RC(check_handle(s));
+    RC(check_single(s));
+    if (!d_xu || !d_xs || !d_goal || !ms_by_kernel || !launches_by_kernel)
+        return fail(GATO_ERR_ARG, "null pointer");
+    RC(bind_device(s));
+    cudaStream_t st = as_stream(stream);
+    std::vector<gato_solver::ProfEntry> entries;
+    s->prof = &entries;
+    std::vector<int> hs(s->B), hc(s->B);
+    int rows = 0;
+    int rc = dispatch(s, [&](auto tg) {
+        using Tg = decltype(tg);
+        if (s->form == GATO_FORM_PLAIN)
+            return solve_plain<Tg>(s, st, d_xu, d_xs, d_goal, hs.data(), hc.data(), &rows);
+        return enqueue_fused<Tg>(s, st, d_xu, d_xs, d_goal);
+    });
+    s->prof = nullptr;
+    cudaError_t e = cudaStreamSynchronize(st);
+    for (int k = 0; k < GATO_KERNEL_COUNT; ++k) {
+        ms_by_kernel[k] = 0.0;
+        launches_by_kernel[k] = 0;
+    }
+    for (auto& en : entries) {
+        float ms = 0.0f;
+        if (rc == 0 && e == cudaSuccess && cudaEventElapsedTime(&ms, en.a, en.b) == cudaSuccess) {
+            ms_by_kernel[en.id] += ms;
+            launches_by_kernel[en.id] += 1;
+        }
+        cudaEventDestroy(en.a);
+        cudaEventDestroy(en.b);
+    }
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(GATO_ERR_CUDA, "profile solve: %s", cudaGetErrorString(e));
+    return GATO_OK;
+}
+
+int gato_set_f_ext_batch(gato_solver_t* s, const float* h_f_ext)
+{
+    RC(check_handle(s));
+    if (!h_f_ext) return fail(GATO_ERR_ARG, "null f_ext");
+    RC(bind_device(s));
+    std::vector<double> v(h_f_ext, h_f_ext + 6 * (size_t)s->B);
+    RC(s->upload(s->fext, v.data(), v.size()));
+    int any = 0;
+    for (double x : v) any |= (x != 0.0);
+    if (any != s->use_fext) {
+        s->use_fext = any;
+        s->version++;
+    }
+    return GATO_OK;
+}
+
+int gato_set_rho_penalty_batch(gato_solver_t* s, const float* h_rho, int set_as_reset_default)
+{
+    RC(check_handle(s));
+    return set_batch(s, s->rho, h_rho, &s->rho_init, set_as_reset_default);
+}
+
+int gato_set_drho_batch(gato_solver_t* s, const float* h_drho, int set_as_reset_default)
+{
+    RC(check_handle(s));
+    RC(set_batch(s, s->drho, h_drho, &s->drho_init, set_as_reset_default));
+    if (set_as_reset_default) RC(s->upload(s->drho_init_d, s->drho_init.data(), s->B));
+    return GATO_OK;
+}
+
+int gato_set_mu_batch(gato_solver_t* s, const float* h_mu)
+{
+    RC(check_handle(s));
+    return set_batch(s, s->mu, h_mu, nullptr, 0);
+}
+
+int gato_set_pcg_tol_batch(gato_solver_t* s, const float* h_tol)
+{
+    RC(check_handle(s));
+    return set_batch(s, s->tol, h_tol, nullptr, 0);
+}
+
+int gato_set_dt(gato_solver_t* s, float dt)
+{
+    RC(check_handle(s));
+    if (!(dt > 0.0f)) return fail(GATO_ERR_ARG, "dt must be positive");
+    if ((double)dt != s->dt) {
+        s->dt = dt;
+        s->version++;
+    }
+    return GATO_OK;
+}
+
+int gato_reset_dual(gato_solver_t* s)
+{
+    RC(check_handle(s));
+    RC(bind_device(s));
+    CK(cudaMemset(s->lambda, 0, s->esz * lambda_count(s)));
+    return GATO_OK;
+}
+
+int gato_reset_rho(gato_solver_t* s)
+{
+    RC(check_handle(s));
+    RC(bind_device(s));
+    RC(s->upload(s->rho, s->rho_init.data(), s->B));
+    RC(s->upload(s->drho, s->drho_init.data(), s->B));
+    return GATO_OK;
+}
+
+int gato_set_rho_adaptation(gato_solver_t* s, int enabled)
+{
+    RC(check_handle(s));
+    if ((enabled != 0) != (s->adapt_rho != 0)) {
+        s->adapt_rho = enabled != 0;
+        s->version++;
+    }
+    return GATO_OK;
+}
+
+int gato_get_lambda(gato_solver_t* s, float* h_lambda)
+{
+    RC(check_handle(s));
+    if (!h_lambda) return fail(GATO_ERR_ARG, "null lambda");
+    RC(bind_device(s));
+    const int n = lambda_count(s);
+    if (s->esz == sizeof(float)) {
+        CK(cudaMemcpy(h_lambda, s->lambda, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<double> t(n);
+        CK(cudaMemcpy(t.data(), s->lambda, sizeof(double) * n, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; ++i) h_lambda[i] = (float)t[i];
+    }
+    return GATO_OK;
+}
+
+int gato_set_lambda(gato_solver_t* s, const float* h_lambda)
+{
+    RC(check_handle(s));
+    if (!h_lambda) return fail(GATO_ERR_ARG, "null lambda");
+    RC(bind_device(s));
+    const int n = lambda_count(s);
+    std::vector<double> t(h_lambda, h_lambda + n);
+    return s->upload(s->lambda, t.data(), n);
+}
+
+int gato_get_lambda_f64(gato_solver_t* s, double* h_lambda)
+{
+    RC(check_handle(s));
+    RC(check_double(s));
+    if (!h_lambda) return fail(GATO_ERR_ARG, "null lambda");
+    RC(bind_device(s));
+    CK(cudaMemcpy(h_lambda, s->lambda, sizeof(double) * lambda_count(s), cudaMemcpyDeviceToHost));
+    return GATO_OK;
+}
+
+int gato_set_lambda_f64(gato_solver_t* s, const double* h_lambda)
+{
+    RC(check_handle(s));
+    RC(check_double(s));
+    if (!h_lambda) return fail(GATO_ERR_ARG, "null lambda");
+    RC(bind_device(s));
+    CK(cudaMemcpy(s->lambda, h_lambda, sizeof(double) * lambda_count(s), cudaMemcpyHostToDevice));
+    return GATO_OK;
+}
+
+int gato_get_rho(gato_solver_t* s, float* h_rho)
+{
+    RC(check_handle(s));
+    if (!h_rho) return fail(GATO_ERR_ARG, "null rho");
+    RC(bind_device(s));
+    if (s->esz == sizeof(float)) {
+        CK(cudaMemcpy(h_rho, s->rho, sizeof(float) * s->B, cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<double> t(s->B);
+        CK(cudaMemcpy(t.data(), s->rho, sizeof(double) * s->B, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < s->B; ++i) h_rho[i] = (float)t[i];
+    }
+    return GATO_OK;
+}
+
+int gato_sim_forward(gato_solver_t* s, const float* h_xk, const float* h_uk, float dt,
+                     float* h_xkp1)
+{
+    RC(check_handle(s));
+    if (!h_xk || !h_uk || !h_xkp1) return fail(GATO_ERR_ARG, "null host buffer");
+    RC(bind_device(s));
+    const int nx = 2 * s->nq, nu = s->nq;
+    cudaStream_t st = s->own_stream;
+    std::vector<double> x(h_xk, h_xk + nx), u(h_uk, h_uk + nu);
+    RC(s->upload(s->sim_x, x.data(), nx));
+    RC(s->upload(s->sim_u, u.data(), nu));
+    RC(dispatch(s, [&](auto tg) {
+        using Tg = decltype(tg);
+        using T = typename Tg::T;
+        const size_t sm = WPB * DynSmem<Tg::NQ>::SIZE * sizeof(T);
+        k_sim_forward<Tg::NQ, T><<<cdiv(s->B, WPB), WPB * WARP, sm, st>>>(
+            dmodel<Tg>(s), s->B, (T)dt, (const T*)s->sim_x, (const T*)s->sim_u, (const T*)s->fext,
+            s->use_fext, (T*)s->sim_out);
+        CKL();
+        return (int)GATO_OK;
+    }));
+    const size_t n = (size_t)nx * s->B;
+    if (s->esz == sizeof(float)) {
+        CK(cudaMemcpyAsync(h_xkp1, s->sim_out, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    } else {
+        std::vector<double> t(n);
+        CK(cudaMemcpyAsync(t.data(), s->sim_out, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (size_t i = 0; i < n; ++i) h_xkp1[i] = (float)t[i];
+    }
+    return GATO_OK;
+}
+
+// --- stage entry points (single-precision solvers) ---------------------------
+int gato_stage_setup_kkt(gato_solver_t* s, void* stream, const float* d_xu, const float* d_xs,
+                         const float* d_goal, float* d_Q, float* d_R, float* d_q, float* d_r,
+                         float* d_A, float* d_B, float* d_c)
+{
+    RC(check_handle(s));
+    RC(check_single(s));
+    RC(bind_device(s));
+    return dispatch(s, [&](auto tg) {
+        using Tg = decltype(tg);
+        using T = typename Tg::T;
+        auto bt = make_batch<Tg>(s, (void*)d_xu, d_xs, d_goal);
+        bt.Q = (T*)d_Q; bt.R = (T*)d_R; bt.q = (T*)d_q; bt.r = (T*)d_r; bt.A = (T*)d_A;
+        bt.Bm = (T*)d_B; bt.c = (T*)d_c;
+        return launch_kkt<Tg>(s, as_stream(stream), bt);
+    });
+}
+
+int gato_stage_form_schur(gato_solver_t* s, void* stream, float* d_Q, float* d_R,
+                          const float* d_q, const float* d_r, const float* d_A, const float* d_B,
+                          const float* d_c, float* d_S, float* d_Pinv, float* d_gamma)
+{
+    RC(check_handle(s));
+    RC(check_single(s));
+    RC(bind_device(s));
+    cudaStream_t st = as_stream(stream);
+    const int nx = 2 * s->nq, nu = s->nq;
+    const size_t nQ = (size_t)s->B * s->N * nx * nx, nR = (size_t)s->B * s->N * nu * nu;
+    RC(dispatch(s, [&](auto tg) {
+        using Tg = decltype(tg);
+        using T = typename Tg::T;
+        auto bt = make_batch<Tg>(s, s->xu, s->xs, s->goal);
+        bt.Q = (T*)d_Q; bt.R = (T*)d_R; bt.q = (T*)d_q; bt.r = (T*)d_r; bt.A = (T*)d_A;
+        bt.Bm = (T*)d_B; bt.c = (T*)d_c; bt.S = (T*)d_S; bt.P = (T*)d_Pinv;
+        bt.gamma = (T*)d_gamma;
+        return launch_schur<Tg>(s, st, bt);
+    }));
+    // the reference leaves (Q + rho I_q)^-1 and R^-1 in d_Q / d_R
+    CK(cudaMemcpyAsync(d_Q, s->Qi, sizeof(float) * nQ, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(d_R, s->Ri, sizeof(float) * nR, cudaMemcpyDeviceToDevice, st));
+    return GATO_OK;
+}
+
+int gato_stage_pcg(gato_solver_t* s, void* stream, const float* d_S, const float* d_Pinv,
+                   const float* d_gamma, float* d_lambda, int32_t* d_iters)
+{
+    RC(check_handle(s));
+    RC(check_single(s));
+    RC(bind_device(s));
+    cudaStream_t st = as_stream(stream);
+    CK(cudaMemsetAsync(s->conv, 0, sizeof(int) * s->B, st));
+    return dispatch(s, [&](auto tg) {
+        using Tg = decltype(tg);
+        using T = typename Tg::T;
+        auto bt = make_batch<Tg>(s, s->xu, s->xs, s->goal);
+        bt.S = (T*)d_S; bt.P = (T*)d_Pinv; bt.gamma = (T*)d_gamma; bt.lambda = (T*)d_lambda;
+        bt.pcg_iters = d_iters;
+        return launch_pcg<Tg>(s, st, bt, -1);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,89 @@
+// Shared device-side definitions: the robot model as a by-value kernel
+// parameter, solver dimensions, and warp helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gato {
+
+constexpr int WARP = 32;
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int NUM_ALPHAS = 8;  // parallel line-search step sizes 2^-j (gato/settings.h:15)
+
+// Penalty adaptation constants of gato/settings.h:17-21 (float in the
+// reference).
+constexpr float RHO_INIT = 1e-3f;
+constexpr float RHO_FACTOR = 1.2f;
+constexpr float RHO_MIN = 1e-8f;
+constexpr float RHO_MAX = 10.0f;
+
+// Robot model for a chain of NQ revolute joints about their local z axes.
+// Built on the host in FP64 from gato_model_t and rounded to FP32.
+//   X_i(q) = rot(Rz(q)^T) * [E0 0; C0 E0]   (motion transform parent -> link)
+//   FK:   T_i = T_{i-1} * [R0 Rz(q) | P]
+template <int NQ, typename T>
+struct DevModel {
+    T E0[NQ][9];   // row-major rotation block of the fixed joint transform
+    T C0[NQ][9];   // row-major coupling block (-E0 * skew(P))
+    T R0[NQ][9];   // row-major joint-frame rotation in the parent (E0^T)
+    T P[NQ][3];    // joint origin in the parent frame
+    T Ibar[NQ][6]; // rotational inertia about the link origin: xx xy xz yy yz zz
+    T h[NQ][3];    // first mass moment m * com
+    T mass[NQ];
+    T qlo[NQ], qhi[NQ], vlo[NQ], vhi[NQ], ulo[NQ], uhi[NQ];
+    T gravity;
+    int barrier_style;  // 0 exact barrier Hessian, 1 outer product of gradients
+};
+
+// Cost weights and time step, as in the BSQP constructor.
+template <typename T>
+struct CostParams {
+    T dt;
+    T q_cost, qd_cost, u_cost, N_cost, q_lim_cost, vel_lim_cost, ctrl_lim_cost;
+};
+
+// precision-generic math
+__device__ __forceinline__ void gsincos(float x, float* s, float* c) { sincosf(x, s, c); }
+__device__ __forceinline__ void gsincos(double x, double* s, double* c) { sincos(x, s, c); }
+__device__ __forceinline__ float glog(float x) { return logf(x); }
+__device__ __forceinline__ double glog(double x) { return log(x); }
+__device__ __forceinline__ float gabs(float x) { return fabsf(x); }
+__device__ __forceinline__ double gabs(double x) { return fabs(x); }
+__device__ __forceinline__ float gmin(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double gmin(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float gmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double gmax(double a, double b) { return fmax(a, b); }
+
+// Per-problem sizes for a plant with NQ joints and horizon N.
+template <int NQ>
+struct Dims {
+    static constexpr int nq = NQ;
+    static constexpr int nx = 2 * NQ;
+    static constexpr int nu = NQ;
+    static constexpr int nxu = nx + nu;
+    static constexpr int nx2 = nx * nx;
+    int N;
+    __host__ __device__ int traj() const { return nxu * N - nu; }
+    __host__ __device__ int vecp() const { return (N + 2) * nx; }   // padded lambda / gamma
+    __host__ __device__ int b3d() const { return 3 * nx2 * N; }     // S / Pinv block rows
+    __host__ __device__ int goal() const { return 6 * N; }
+};
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
+
+__device__ __forceinline__ float warp_sum(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+}  // namespace gato

@@ -1,0 +1,557 @@
+// Batched kernels of the SQP solve.
+//
+// Plain form: one launch per stage with the reference's data flow through
+// global memory (gato/bsqp/kernels/*.cuh).  Fused form: one block per problem
+// runs KKT set-up -> Schur -> PCG -> step recovery without leaving the SM,
+// with S and P^-1 resident in shared memory, and a second block-per-problem
+// kernel runs the merit evaluation and line search; convergence bookkeeping
+// stays on the device so that a whole solve is one CUDA graph.
+#pragma once
+
+#include "common.cuh"
+#include "dynamics.cuh"
+#include "stages.cuh"
+
+namespace gato {
+
+// Per-solver device state handed to every kernel by value.
+template <int NQ, typename T>
+struct Batch {
+    int B, N;
+    float solve_ratio;
+    int max_pcg_iters;
+    int adapt_rho;
+    CostParams<T> cp;
+    // problem data
+    T* xu;
+    const T* xs;
+    const T* goal;
+    const T* fext;         // [B][6]
+    int use_fext;          // 0: f_ext all zero, skip the wrench terms
+    // KKT system and Schur complement
+    T *Q, *R, *q, *r, *A, *Bm, *c, *Qi, *Ri;
+    T *S, *P, *gamma, *lambda, *dz;
+    // per-problem scalars
+    T *rho, *drho, *mu, *tol;
+    double *merit_terms;   // [B][NUM_ALPHAS][N]
+    double *merit_init, *merit_init0, *merit_final;
+    int *pcg_iters, *conv, *sqp_iters;
+    int* done;             // device flag: batch converged (fused form)
+    int* ls_count;         // line-search iterations run (fused form)
+    // per-iteration statistics [iter][B]
+    int* h_pcg;
+    float *h_ls_min, *h_ls_step;
+};
+
+// ------------------------------------------------------------------ merit
+// One warp per (knot, alpha); terms[b][alpha][k].
+template <int NQ, typename T>
+__global__ void k_merit(Batch<NQ, T> bt, DevModel<NQ, T> M, int nalpha, int use_dz, int skip_if_done)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
+    if (skip_if_done && *bt.done) return;
+    const int b = blockIdx.y;
+    const int wpb = blockDim.x / WARP;
+    const int item = blockIdx.x * wpb + warp_id();
+    const int N = bt.N;
+    if (item >= N * nalpha) return;
+    const int k = item % N, j = item / N;
+    T* s = smem + warp_id() * MeritSmem<NQ>::SIZE;
+    const Dims<NQ> d{N};
+    const T alpha = T(1) / (T)(1 << j);
+    const T v = merit_knot<NQ, T>(M, bt.cp, N, k, alpha, bt.mu[b], bt.xu + (size_t)b * d.traj(),
+                                   use_dz ? bt.dz + (size_t)b * d.traj() : nullptr,
+                                   bt.xs + (size_t)b * Dims<NQ>::nx, bt.goal + (size_t)b * d.goal(),
+                                   bt.use_fext ? bt.fext + 6 * b : nullptr, s);
+    if (lane_id() == 0) bt.merit_terms[((size_t)b * NUM_ALPHAS + j) * N + k] = (double)v;
+}
+
+// Sum of the alpha = 1 terms into out[b] (initial / final merit).
+template <typename Acc>
+__global__ void k_merit_sum(int B, int N, const double* terms, double* out, double* out2)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    Acc s = 0;
+    for (int k = 0; k < N; ++k) s += (Acc)terms[(size_t)b * NUM_ALPHAS * N + k];
+    out[b] = (double)s;
+    if (out2) out2[b] = (double)s;
+}
+
+// ------------------------------------------------------------------ line search
+// lineSearchAndUpdateBatchedKernel (gato/bsqp/kernels/line_search.cuh:12-98),
+// one block per problem.  Merit sums over knots are formed here in a fixed
+// order (Acc precision) instead of the reference's float atomicAdd.
+template <int NQ, typename T, typename Acc>
+__global__ void k_line_search(Batch<NQ, T> bt, int it, int skip_if_done)
+{
+    if (skip_if_done && *bt.done) return;
+    const int b = blockIdx.x;
+    const int N = bt.N;
+    __shared__ Acc s_m[NUM_ALPHAS];
+    __shared__ T s_step;
+    __shared__ int s_ok;
+    const int t = threadIdx.x;
+    if (t < NUM_ALPHAS) {
+        Acc s = 0;
+        const double* tm = bt.merit_terms + ((size_t)b * NUM_ALPHAS + t) * N;
+        for (int k = 0; k < N; ++k) s += (Acc)tm[k];
+        s_m[t] = s;
+    }
+    __syncthreads();
+    if (t == 0) {
+        Acc best = (Acc)1e38;
+        int bj = 0;
+        for (int j = 0; j < NUM_ALPHAS; ++j)
+            if (s_m[j] < best) {
+                best = s_m[j];
+                bj = j;
+            }
+        const Acc m0 = (Acc)bt.merit_init[b];
+        const bool ok = best < m0;
+        if (bt.adapt_rho) {
+            const T dr = bt.drho[b];
+            const T fac = T(RHO_FACTOR);
+            const T mult = ok ? gmin(dr / fac, T(1) / fac) : gmax(dr * fac, fac);
+            bt.drho[b] = mult;
+            const T rr = gmax(bt.rho[b] * mult, T(RHO_MIN));
+            bt.rho[b] = gmin(rr, T(RHO_MAX));
+        }
+        T step;
+        if (!ok) {
+            if (bt.rho[b] > T(RHO_MAX)) bt.rho[b] = T(RHO_INIT);
+            step = T(-1);
+        } else {
+            step = T(1) / (T)(1 << bj);
+            bt.merit_init[b] = (double)best;
+        }
+        s_step = step;
+        s_ok = ok;
+        if (bt.h_ls_min) {
+            bt.h_ls_min[(size_t)it * bt.B + b] = (float)bt.merit_init[b];
+            bt.h_ls_step[(size_t)it * bt.B + b] = (float)step;
+        }
+    }
+    __syncthreads();
+    if (s_ok) {
+        const Dims<NQ> d{N};
+        T* x = bt.xu + (size_t)b * d.traj();
+        const T* dz = bt.dz + (size_t)b * d.traj();
+        const T st = s_step;
+        for (int i = t; i < d.traj(); i += blockDim.x) x[i] += st * dz[i];
+    }
+}
+
+// ------------------------------------------------------------------ KKT
+template <int NQ, typename T>
+__global__ void k_kkt(Batch<NQ, T> bt, DevModel<NQ, T> M)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
+    const int b = blockIdx.y;
+    const int wpb = blockDim.x / WARP;
+    const int k = blockIdx.x * wpb + warp_id();
+    const int N = bt.N;
+    if (k >= N - 1) return;
+    const Dims<NQ> d{N};
+    constexpr int nx = Dims<NQ>::nx, nu = Dims<NQ>::nu;
+    T* s = smem + warp_id() * KktSmem<NQ>::SIZE;
+    kkt_knot<NQ, T>(M, bt.cp, N, k, bt.xu + (size_t)b * d.traj(), bt.xs + (size_t)b * nx,
+                 bt.goal + (size_t)b * d.goal(), bt.use_fext ? bt.fext + 6 * b : nullptr,
+                 bt.Q + (size_t)b * N * nx * nx, bt.R + (size_t)b * N * nu * nu,
+                 bt.q + (size_t)b * N * nx, bt.r + (size_t)b * N * nu,
+                 bt.A + (size_t)b * N * nx * nx, bt.Bm + (size_t)b * N * nx * nu,
+                 bt.c + (size_t)b * N * nx, s);
+}
+
+// ------------------------------------------------------------------ Schur
+// Inverses Qi_k = (Q_k + rho I_q)^-1 (all k) and Ri_k = R_k^-1 (k < N-1),
+// one warp per knot.
+template <int NQ, typename T>
+__global__ void k_schur_inv(Batch<NQ, T> bt)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
+    const int b = blockIdx.y;
+    const int wpb = blockDim.x / WARP;
+    const int k = blockIdx.x * wpb + warp_id();
+    const int N = bt.N;
+    if (k >= N) return;
+    constexpr int nx = Dims<NQ>::nx, nu = Dims<NQ>::nu;
+    const T rho = bt.rho[b];
+    const T* Qk = bt.Q + ((size_t)b * N + k) * nx * nx;
+    warp_invert<nx, T>(Qk, rho, bt.Qi + ((size_t)b * N + k) * nx * nx);
+    if (k < N - 1) warp_invert<nu, T>(bt.R + ((size_t)b * N + k) * nu * nu, 0.0f,
+                                   bt.Ri + ((size_t)b * N + k) * nu * nu);
+}
+
+template <int NQ, typename T>
+__global__ void k_schur(Batch<NQ, T> bt)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
+    const int b = blockIdx.y;
+    const int wpb = blockDim.x / WARP;
+    const int k = blockIdx.x * wpb + warp_id();
+    const int N = bt.N;
+    if (k >= N) return;
+    const Dims<NQ> d{N};
+    constexpr int nx = Dims<NQ>::nx, nu = Dims<NQ>::nu;
+    T* S = bt.S + (size_t)b * d.b3d();
+    T* P = bt.P + (size_t)b * d.b3d();
+    T* g = bt.gamma + (size_t)b * d.vecp();
+    const T* Qi = bt.Qi + (size_t)b * N * nx * nx;
+    if (k == N - 1) {
+        schur_first<NQ, T>(bt.rho[b], bt.Q + (size_t)b * N * nx * nx, Qi, bt.q + (size_t)b * N * nx,
+                        bt.c + (size_t)b * N * nx, S, P, g);
+        return;
+    }
+    T* s = smem + warp_id() * SchurSmem<NQ>::SIZE;
+    schur_knot<NQ, T>(k, bt.rho[b], Qi, bt.Ri + (size_t)b * N * nu * nu, bt.q + (size_t)b * N * nx,
+                   bt.r + (size_t)b * N * nu, bt.A + (size_t)b * N * nx * nx,
+                   bt.Bm + (size_t)b * N * nx * nu, bt.c + (size_t)b * N * nx, S, P, g, s);
+}
+
+template <int NQ, typename T>
+__global__ void k_schur_off(Batch<NQ, T> bt)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
+    const int b = blockIdx.y;
+    const int wpb = blockDim.x / WARP;
+    const int k = blockIdx.x * wpb + warp_id();
+    const int N = bt.N;
+    if (k >= N - 1) return;
+    const Dims<NQ> d{N};
+    constexpr int nx = Dims<NQ>::nx;
+    T* s = smem + warp_id() * 4 * nx * nx;
+    schur_offdiag<NQ, T>(k, bt.S + (size_t)b * d.b3d(), bt.P + (size_t)b * d.b3d(), s);
+}
+
+// ------------------------------------------------------------------ PCG
+// Block-tridiagonal matrix-vector product over padded vectors
+// (btdMatrixVectorProduct, gato/utils/linalg.cuh:174-221): warp w takes block
+// rows w, w+W, ...; lane 2*row+half sums half of the 3n columns of one row.
+// Returns this lane's partial of out . dotw over the entries it wrote.
+template <int NQ, typename T, typename Acc>
+__device__ __forceinline__ Acc btd_mv(int N, const T* __restrict__ Mx, const T* __restrict__ vin,
+                                      T* __restrict__ vout, const T* __restrict__ dotw)
+{
+    constexpr int n = 2 * NQ, RD = 3 * n, HALF = RD / 2;
+    const int l = lane_id();
+    const int row = l >> 1, half = l & 1;
+    const int nw = blockDim.x / WARP;
+    Acc part = 0;
+    for (int br = warp_id(); br < N; br += nw) {
+        T acc = T(0);
+        if (row < n) {
+            const T* mrow = Mx + (size_t)br * n * RD + row * RD + half * HALF;
+            const T* v = vin + br * n + half * HALF;
+#pragma unroll
+            for (int c = 0; c < HALF; ++c) acc += mrow[c] * v[c];
+        }
+        acc += __shfl_xor_sync(FULL, acc, 1);
+        if (row < n && half == 0) {
+            const int idx = (br + 1) * n + row;
+            vout[idx] = acc;
+            part += (Acc)acc * (Acc)dotw[idx];
+        }
+    }
+    return part;
+}
+
+template <typename Acc>
+__device__ __forceinline__ Acc block_sum(Acc v, Acc* red)
+{
+    v = warp_sum(v);
+    if (lane_id() == 0) red[warp_id()] = v;
+    __syncthreads();
+    Acc s = 0;
+    const int nw = blockDim.x / WARP;
+    for (int w = 0; w < nw; ++w) s += red[w];
+    return s;
+}
+
+// Preconditioned CG on S lambda = gamma for one problem, one block
+// (solvePCGBatchedKernel, gato/bsqp/kernels/pcg.cuh:23-147): warm start from
+// lambda, stop when |r.z| < 1e-6 + eps |r0.z0|, zero iterations (lambda left
+// untouched) when |r0.z0| < 1e-6.  S and P may live in shared or global
+// memory.  sv holds 5 padded vectors, red 2*32 Acc.  Returns the iteration
+// count.
+template <int NQ, typename T, typename Acc>
+__device__ int pcg_block(int N, const T* __restrict__ S, const T* __restrict__ P,
+                         const T* __restrict__ gamma, T* __restrict__ lam, T eps, int max_iters,
+                         T* sv, Acc* red)
+{
+    constexpr int n = 2 * NQ;
+    const int L = (N + 2) * n;
+    const int tid = threadIdx.x, bs = blockDim.x;
+    T* x = sv;
+    T* r = x + L;
+    T* z = r + L;
+    T* p = z + L;
+    T* Ap = p + L;
+    for (int i = tid; i < L; i += bs) {
+        x[i] = lam[i];
+        r[i] = 0.0f;
+        z[i] = 0.0f;
+        p[i] = 0.0f;
+        Ap[i] = 0.0f;
+    }
+    __syncthreads();
+    btd_mv<NQ, T, Acc>(N, S, x, r, r);
+    __syncthreads();
+    for (int i = tid; i < L; i += bs) r[i] = gamma[i] - r[i];
+    __syncthreads();
+    Acc part = btd_mv<NQ, T, Acc>(N, P, r, z, r);
+    Acc rho = block_sum<Acc>(part, red);
+    for (int i = tid; i < L; i += bs) p[i] = z[i];
+    const Acc abs_tol = Acc(1e-6);
+    if (fabs((double)rho) < (double)abs_tol) return 0;
+    const Acc rho_init = rho < 0 ? -rho : rho;
+    __syncthreads();
+    int it = 0;
+    for (int i = 0; i < max_iters; ++i) {
+        ++it;
+        part = btd_mv<NQ, T, Acc>(N, S, p, Ap, p);
+        const Acc pAp = block_sum<Acc>(part, red);
+        const Acc alpha = rho / pAp;
+        const T af = (T)alpha;
+        for (int j = tid; j < L; j += bs) {
+            x[j] += af * p[j];
+            r[j] -= af * Ap[j];
+        }
+        __syncthreads();
+        part = btd_mv<NQ, T, Acc>(N, P, r, z, r);
+        const Acc rho_new = block_sum<Acc>(part, red + WARP);
+        const Acc arn = rho_new < 0 ? -rho_new : rho_new;
+        if (arn < abs_tol + (Acc)eps * rho_init) break;
+        const Acc beta = rho_new / rho;
+        rho = rho_new;
+        const T bf = (T)beta;
+        for (int j = tid; j < L; j += bs) p[j] = z[j] + bf * p[j];
+        __syncthreads();
+    }
+    __syncthreads();
+    for (int i = tid; i < L; i += bs) lam[i] = x[i];
+    return it;
+}
+
+// Dynamic shared memory of k_pcg: matrices staged when `stage` is set.
+// Layout: [S | P (when staged) | 5 padded vectors | reduction slots].
+template <int NQ, typename T>
+__host__ __device__ inline size_t pcg_smem_bytes(int N, bool stage)
+{
+    const Dims<NQ> d{N};
+    size_t f = 5 * (size_t)d.vecp() + (stage ? 2 * (size_t)d.b3d() : 0);
+    return f * sizeof(T) + 2 * WARP * sizeof(double) + 32;
+}
+
+template <int NQ, typename T, typename Acc>
+__global__ void k_pcg(Batch<NQ, T> bt, int stage, int it_row)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
+    const int b = blockIdx.x;
+    const Dims<NQ> d{bt.N};
+    int iters = 0;
+    if (!bt.conv[b]) {
+        const T* S = bt.S + (size_t)b * d.b3d();
+        const T* P = bt.P + (size_t)b * d.b3d();
+        const size_t mats = stage ? 2 * (size_t)d.b3d() : 0;
+        T* sv = smem + mats;
+        Acc* red = reinterpret_cast<Acc*>(
+            ((uintptr_t)(smem + mats + 5 * d.vecp()) + 15) & ~(uintptr_t)15);
+        if (stage) {
+            T* sS = smem;
+            T* sP = sS + d.b3d();
+            const uint4* gS = reinterpret_cast<const uint4*>(S);
+            const uint4* gP = reinterpret_cast<const uint4*>(P);
+            uint4* tS = reinterpret_cast<uint4*>(sS);
+            uint4* tP = reinterpret_cast<uint4*>(sP);
+            const int chunks = (int)((size_t)d.b3d() * sizeof(T) / sizeof(uint4));
+            for (int i = threadIdx.x; i < chunks; i += blockDim.x) {
+                tS[i] = gS[i];
+                tP[i] = gP[i];
+            }
+            __syncthreads();
+            S = sS;
+            P = sP;
+        }
+        iters = pcg_block<NQ, T, Acc>(bt.N, S, P, bt.gamma + (size_t)b * d.vecp(),
+                                   bt.lambda + (size_t)b * d.vecp(), bt.tol[b], bt.max_pcg_iters,
+                                   sv, red);
+    }
+    if (threadIdx.x == 0) {
+        bt.pcg_iters[b] = iters;
+        if (it_row >= 0 && bt.h_pcg) bt.h_pcg[(size_t)it_row * bt.B + b] = iters;
+    }
+}
+
+// ------------------------------------------------------------------ dz
+template <int NQ, typename T>
+__global__ void k_dz(Batch<NQ, T> bt)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
+    const int b = blockIdx.y;
+    const int wpb = blockDim.x / WARP;
+    const int k = blockIdx.x * wpb + warp_id();
+    const int N = bt.N;
+    if (k >= N) return;
+    const Dims<NQ> d{N};
+    constexpr int nx = Dims<NQ>::nx, nu = Dims<NQ>::nu;
+    T* s = smem + warp_id() * 3 * nx;
+    dz_knot<NQ, T>(N, k, bt.lambda + (size_t)b * d.vecp(), bt.Qi + (size_t)b * N * nx * nx,
+                bt.Ri + (size_t)b * N * nu * nu, bt.q + (size_t)b * N * nx,
+                bt.r + (size_t)b * N * nu, bt.A + (size_t)b * N * nx * nx,
+                bt.Bm + (size_t)b * N * nx * nu, bt.dz + (size_t)b * d.traj(), s);
+}
+
+// ------------------------------------------------------------------ fused
+// Convergence bookkeeping of one SQP iteration, one block
+// (gato/bsqp/bsqp.cuh:141-167 run on the device): a problem whose PCG took
+// zero iterations is converged; the batch is done once the converged count
+// reaches B * solve_ratio.
+template <int NQ, typename T>
+__global__ void k_check(Batch<NQ, T> bt)
+{
+    __shared__ int s_count;
+    if (threadIdx.x == 0) s_count = 0;
+    __syncthreads();
+    if (*bt.done) return;
+    int local = 0;
+    for (int b = threadIdx.x; b < bt.B; b += blockDim.x) {
+        int cv = bt.conv[b];
+        int si = bt.sqp_iters[b];
+        if (bt.pcg_iters[b] == 0) {
+            cv = 1;
+            si += 1;
+        }
+        if (cv) local++;
+        else si += 1;
+        bt.conv[b] = cv;
+        bt.sqp_iters[b] = si;
+    }
+    atomicAdd(&s_count, local);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if ((float)s_count >= (float)bt.B * bt.solve_ratio) *bt.done = 1;
+        else *bt.ls_count += 1;
+    }
+}
+
+// Shared memory of the fused SQP-iteration kernel.
+template <int NQ, typename T>
+struct FusedLayout {
+    int N, warps;
+    bool stage;  // S and P^-1 resident in shared memory
+    __host__ __device__ size_t scratch_floats() const
+    {
+        int a = KktSmem<NQ>::SIZE, bsz = SchurSmem<NQ>::SIZE, c = 4 * (2 * NQ) * (2 * NQ);
+        int m = a > bsz ? a : bsz;
+        m = m > c ? m : c;
+        return (size_t)warps * m;
+    }
+    __host__ __device__ size_t mats_floats() const
+    {
+        const Dims<NQ> d{N};
+        return stage ? 2 * (size_t)d.b3d() : 0;
+    }
+    __host__ __device__ size_t vec_floats() const
+    {
+        const Dims<NQ> d{N};
+        return 5 * (size_t)d.vecp();
+    }
+    __host__ __device__ size_t bytes() const
+    {
+        // scratch and the PCG vectors are not live at the same time
+        size_t s = scratch_floats(), v = vec_floats();
+        return (mats_floats() + (s > v ? s : v)) * sizeof(T) + 2 * WARP * sizeof(double) + 16;
+    }
+};
+
+// One SQP iteration of one problem up to the step (KKT set-up, Schur
+// complement, PCG, step recovery), one block.
+template <int NQ, typename T, typename Acc>
+__global__ void k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int it_row)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
+    if (*bt.done) return;
+    const int b = blockIdx.x;
+    const int N = bt.N;
+    const Dims<NQ> d{N};
+    constexpr int nx = Dims<NQ>::nx, nu = Dims<NQ>::nu;
+    const int nw = blockDim.x / WARP;
+    FusedLayout<NQ, T> lay{N, nw, stage != 0};
+    T* mats = smem;
+    T* work = smem + lay.mats_floats();
+    const size_t sc = lay.scratch_floats() / nw;
+    T* ws = work + warp_id() * sc;
+    size_t wfl = lay.scratch_floats() > lay.vec_floats() ? lay.scratch_floats() : lay.vec_floats();
+    Acc* red = reinterpret_cast<Acc*>(((uintptr_t)(work + wfl) + 15) & ~(uintptr_t)15);
+
+    T* Q = bt.Q + (size_t)b * N * nx * nx;
+    T* R = bt.R + (size_t)b * N * nu * nu;
+    T* qv = bt.q + (size_t)b * N * nx;
+    T* rv = bt.r + (size_t)b * N * nu;
+    T* A = bt.A + (size_t)b * N * nx * nx;
+    T* Bm = bt.Bm + (size_t)b * N * nx * nu;
+    T* c = bt.c + (size_t)b * N * nx;
+    T* Qi = bt.Qi + (size_t)b * N * nx * nx;
+    T* Ri = bt.Ri + (size_t)b * N * nu * nu;
+    T* S = stage ? mats : bt.S + (size_t)b * d.b3d();
+    T* P = stage ? mats + d.b3d() : bt.P + (size_t)b * d.b3d();
+    T* g = bt.gamma + (size_t)b * d.vecp();
+    const T rho = bt.rho[b];
+    const T* xu = bt.xu + (size_t)b * d.traj();
+    const T* fext = bt.use_fext ? bt.fext + 6 * b : nullptr;
+
+    for (int k = warp_id(); k < N - 1; k += nw)
+        kkt_knot<NQ, T>(M, bt.cp, N, k, xu, bt.xs + (size_t)b * nx, bt.goal + (size_t)b * d.goal(),
+                     fext, Q, R, qv, rv, A, Bm, c, ws);
+    __syncthreads();
+    for (int k = warp_id(); k < N; k += nw) {
+        warp_invert<nx, T>(Q + k * nx * nx, rho, Qi + k * nx * nx);
+        if (k < N - 1) warp_invert<nu, T>(R + k * nu * nu, T(0), Ri + k * nu * nu);
+    }
+    if (stage) {
+        // the padding blocks of S and P^-1 (row 0 left, row N-1 right) are zero
+        for (int i = threadIdx.x; i < nx * 3 * nx; i += blockDim.x) {
+            const int y = i / (3 * nx), x = i % (3 * nx);
+            if (x < nx) {
+                S[y * 3 * nx + x] = 0.0f;
+                P[y * 3 * nx + x] = 0.0f;
+            } else if (x >= 2 * nx) {
+                S[(size_t)(N - 1) * 3 * nx * nx + y * 3 * nx + x] = 0.0f;
+                P[(size_t)(N - 1) * 3 * nx * nx + y * 3 * nx + x] = 0.0f;
+            }
+        }
+    }
+    __syncthreads();
+    for (int k = warp_id(); k < N; k += nw) {
+        if (k == N - 1)
+            schur_first<NQ, T>(rho, Q, Qi, qv, c, S, P, g);
+        else
+            schur_knot<NQ, T>(k, rho, Qi, Ri, qv, rv, A, Bm, c, S, P, g, ws);
+    }
+    __syncthreads();
+    for (int k = warp_id(); k < N - 1; k += nw) schur_offdiag<NQ, T>(k, S, P, ws);
+    __syncthreads();
+    int iters = 0;
+    if (!bt.conv[b])
+        iters = pcg_block<NQ, T, Acc>(N, S, P, g, bt.lambda + (size_t)b * d.vecp(), bt.tol[b],
+                                   bt.max_pcg_iters, work, red);
+    __syncthreads();
+    for (int k = warp_id(); k < N; k += nw)
+        dz_knot<NQ, T>(N, k, bt.lambda + (size_t)b * d.vecp(), Qi, Ri, qv, rv, A, Bm,
+                    bt.dz + (size_t)b * d.traj(), ws);
+    if (threadIdx.x == 0) {
+        bt.pcg_iters[b] = iters;
+        if (bt.h_pcg) bt.h_pcg[(size_t)it_row * bt.B + b] = iters;
+    }
+}
+
+}  // namespace gato

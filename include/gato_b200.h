@@ -57,8 +57,11 @@ enum {
 /* Arithmetic of the device path. */
 enum {
     GATO_PREC_FP32 = 0,   /* everything FP32 (the reference's arithmetic) */
-    GATO_PREC_MIXED = 1   /* FP32 math, FP64 PCG inner products, alpha/beta
+    GATO_PREC_MIXED = 1,  /* FP32 math, FP64 PCG inner products, alpha/beta
                              recurrences and merit reductions */
+    GATO_PREC_FP64 = 2    /* everything FP64 (the reference's USE_DOUBLES build,
+                             gato/settings.h:7-11, python/bindings.cu:244-252);
+                             solves take double buffers (the _f64 entry points) */
 };
 
 /*
@@ -170,7 +173,37 @@ int gato_solve(gato_solver_t* s, void* stream, float* d_xu, const float* d_xs,
 int gato_solve_host(gato_solver_t* s, float* h_xu, float dt, const float* h_xs,
                     const float* h_goal, gato_stats_t* stats);
 
-/* Batched setters (host arrays of B floats, or 6*B for f_ext).
+/* The two solves above for GATO_PREC_FP64 solvers (double buffers), as the
+   BSQP_{B}_double classes of the reference's USE_DOUBLES build. */
+int gato_solve_f64(gato_solver_t* s, void* stream, double* d_xu, const double* d_xs,
+                   const double* d_goal, gato_stats_t* stats);
+int gato_solve_host_f64(gato_solver_t* s, double* h_xu, double dt, const double* h_xs,
+                        const double* h_goal, gato_stats_t* stats);
+
+/* Kernel groups reported by gato_profile_solve. */
+enum {
+    GATO_KERNEL_KKT = 0,
+    GATO_KERNEL_SCHUR = 1,
+    GATO_KERNEL_PCG = 2,
+    GATO_KERNEL_DZ = 3,
+    GATO_KERNEL_MERIT = 4,
+    GATO_KERNEL_LINE_SEARCH = 5,
+    GATO_KERNEL_FUSED_ITER = 6,
+    GATO_KERNEL_CHECK = 7,
+    GATO_KERNEL_MERIT_SUM = 8,
+    GATO_KERNEL_COUNT = 9
+};
+
+/* Runs one solve like gato_solve (fused form without its CUDA graph) and
+   brackets every kernel launch with CUDA events on `stream`; fills
+   ms_by_kernel / launches_by_kernel [GATO_KERNEL_COUNT] with the summed
+   device time and launch count per kernel group, and synchronises the stream.
+   The reference only times the whole solve on the host (bsqp.cuh:109-190). */
+int gato_profile_solve(gato_solver_t* s, void* stream, float* d_xu, const float* d_xs,
+                       const float* d_goal, double* ms_by_kernel, int32_t* launches_by_kernel);
+
+/* Batched setters (host arrays of B floats, or 6*B for f_ext; FP64 solvers
+   widen them).
    Replace BSQP::set_f_ext_batch / set_rho_penalty_batch / set_drho_batch /
    set_mu_batch / set_pcg_tol_batch (gato/bsqp/bsqp.cuh:63-83) and their
    bindings (python/bindings.cu:150-178). */
@@ -199,6 +232,8 @@ int gato_set_rho_adaptation(gato_solver_t* s, int enabled);
    (host memory).  The reference keeps it device-internal (bsqp.cuh:81). */
 int gato_get_lambda(gato_solver_t* s, float* h_lambda);
 int gato_set_lambda(gato_solver_t* s, const float* h_lambda);
+int gato_get_lambda_f64(gato_solver_t* s, double* h_lambda);
+int gato_set_lambda_f64(gato_solver_t* s, const double* h_lambda);
 /* Copies the current penalty rho [B] out (host memory). */
 int gato_get_rho(gato_solver_t* s, float* h_rho);
 

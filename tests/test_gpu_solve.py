@@ -1,0 +1,196 @@
+"""Solve-level parity of the CUDA solver with the FP64 oracle through the
+C ABI.
+
+  * FP64 device arithmetic (the reference's USE_DOUBLES build) reproduces the
+    oracle exactly: identical SQP / PCG iteration counts and line-search
+    steps, trajectories within 1e-8 (normalised).
+  * FP32 (the reference's arithmetic): a single SQP iteration from identical
+    inputs matches the oracle's iteration counts and its trajectory within the
+    FP32 tolerance stated in each test.
+  * The plain and fused forms are bitwise identical.
+"""
+import numpy as np
+import pytest
+
+from helpers import PARAMS_CFG1, PARAMS_CFG2, gpu_solver, nerr, oracle_params, problem
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def cuda():
+    import torch
+    assert torch.cuda.is_available()
+    torch.cuda.set_device(0)
+
+
+def run_pair(O, plant, N, B, params, form, precision, seed, perturbed=True, goals="figure8",
+             lam=None):
+    pr = problem(plant, N, B, seed, perturbed=perturbed, goals=goals)
+    s = gpu_solver(plant, N, B, form=form, precision=precision, **params)
+    ref = O.Solver(plant, N, B, oracle_params(O, **params), threads=4)
+    if lam is not None:
+        s.set_lambda(lam)
+        ref.set_lambda(lam)
+    g = s.solve_raw(pr["xu"], 0.01, pr["xs"], pr["goal"])
+    xo, so = ref.solve(pr["xu"].astype(np.float64), 0.01, pr["xs"], pr["goal"])
+    out = dict(g=g, o=so, xo=xo, lam_g=s.get_lambda(), lam_o=ref.get_lambda(),
+               rho_g=s.get_rho(), rho_o=ref.get_rho())
+    s.close()
+    return out
+
+
+@pytest.mark.parametrize("plant,N,form", [("iiwa14", 8, "fused"), ("iiwa14", 32, "fused"),
+                                          ("iiwa14", 32, "plain"), ("indy7", 32, "fused")])
+def test_fp64_solve_reproduces_oracle(oracle_mod, plant, N, form):
+    r = run_pair(oracle_mod, plant, N, 4, PARAMS_CFG2, form, "fp64", seed=31)
+    g, o = r["g"], r["o"]
+    assert g["ls_num_iters"] == o["ls_num_iters"]
+    np.testing.assert_array_equal(g["pcg_iters"], o["pcg_iters"])
+    np.testing.assert_array_equal(g["sqp_iters"], o["sqp_iters"])
+    np.testing.assert_array_equal(g["kkt_converged"], o["kkt_converged"])
+    np.testing.assert_array_equal(g["ls_step_size"], o["ls_step_size"].astype(np.float32))
+    assert nerr(g["XU"], r["xo"]) < 1e-8
+    assert nerr(r["lam_g"], r["lam_o"]) < 1e-6
+    np.testing.assert_allclose(g["final_merit"], o["final_merit"], rtol=1e-6)
+    np.testing.assert_allclose(r["rho_g"], r["rho_o"], rtol=1e-6)
+
+
+def test_fp64_interface_defaults_reproduce_oracle(oracle_mod):
+    """rho = 0, the interface default (python/bsqp/interface.py:26)."""
+    params = dict(max_sqp_iters=4, pcg_tol=1e-5, max_pcg_iters=173)
+    r = run_pair(oracle_mod, "iiwa14", 32, 3, params, "fused", "fp64", seed=8)
+    np.testing.assert_array_equal(r["g"]["pcg_iters"], r["o"]["pcg_iters"])
+    assert nerr(r["g"]["XU"], r["xo"]) < 1e-8
+
+
+def test_fp64_batch_convergence_semantics(oracle_mod):
+    """Problems whose warm start already solves the QP converge (PCG takes
+    zero iterations) while others continue; the batch keeps iterating, with
+    the reference's per-problem sqp_iters / kkt_converged bookkeeping."""
+    O = oracle_mod
+    plant, N, B = "iiwa14", 16, 6
+    params = dict(PARAMS_CFG2, max_sqp_iters=12)
+    pr = problem(plant, N, B, seed=12, perturbed=False, goals="constant")
+    # converge every problem once, then perturb half of them
+    s = gpu_solver(plant, N, B, precision="fp64", **dict(params, max_sqp_iters=40))
+    res = s.solve_raw(pr["xu"], 0.01, pr["xs"], pr["goal"])
+    lam = s.get_lambda()
+    s.close()
+    xu = res["XU"].copy()
+    rng = np.random.default_rng(3)
+    xu[::2, 14:] += rng.normal(0, 0.02, xu[::2, 14:].shape)
+    s = gpu_solver(plant, N, B, precision="fp64", **params)
+    ref = O.Solver(plant, N, B, oracle_params(O, **params))
+    s.set_lambda(lam)
+    ref.set_lambda(lam)
+    g = s.solve_raw(xu, 0.01, pr["xs"], pr["goal"])
+    xo, so = ref.solve(xu, 0.01, pr["xs"], pr["goal"])
+    s.close()
+    assert so["kkt_converged"].any(), "case must contain converged problems"
+    np.testing.assert_array_equal(g["kkt_converged"], so["kkt_converged"])
+    np.testing.assert_array_equal(g["sqp_iters"], so["sqp_iters"])
+    np.testing.assert_array_equal(g["pcg_iters"], so["pcg_iters"])
+    assert g["ls_num_iters"] == so["ls_num_iters"]
+    assert nerr(g["XU"], xo) < 1e-8
+
+
+@pytest.mark.parametrize("form,precision", [("fused", "fp32"), ("plain", "fp32"),
+                                            ("fused", "mixed"), ("plain", "mixed")])
+def test_config1_single_iteration(oracle_mod, form, precision):
+    """iiwa14, N=8, batch 1, constant goal, default warm start, 1 SQP
+    iteration, PCG tol 1e-5; FP32 device arithmetic.  Tolerance: equal
+    iteration counts and steps, XU within 1e-4 (normalised by max |XU|)."""
+    r = run_pair(oracle_mod, "iiwa14", 8, 1, PARAMS_CFG1, form, precision, seed=1,
+                 perturbed=False, goals="constant")
+    g, o = r["g"], r["o"]
+    np.testing.assert_array_equal(g["pcg_iters"], o["pcg_iters"])
+    np.testing.assert_array_equal(g["ls_step_size"], o["ls_step_size"].astype(np.float32))
+    assert nerr(g["XU"], r["xo"]) < 1e-4
+    np.testing.assert_allclose(g["final_merit"], o["final_merit"], rtol=1e-4)
+
+
+def test_fp32_stepwise_parity_n32(oracle_mod):
+    """iiwa14 N=32 (the benchmark configuration), batch 8: five SQP
+    iterations, each run once on the GPU (FP32) and once in the oracle (FP64)
+    from the identical state (XU, lambda, rho).  FP32 tolerance: at least 85%
+    of the (problem, iteration) PCG counts equal and all within 15%; where the
+    step matches, XU within 5e-3 (normalised) with a median within 1e-3.
+    The bound comes from the PCG stopping rule, not from FP32 alone:
+    |r.z| < 1e-6 + 1e-5 |r0.z0| leaves a preconditioned residual of about
+    sqrt(1e-5) = 3e-3 of the initial one, so two solves that round differently
+    stop at multipliers about 1e-3 apart (the FP64 device mode, which rounds
+    like the oracle, agrees to 1e-8)."""
+    O = oracle_mod
+    plant, N, B = "iiwa14", 32, 8
+    params = dict(PARAMS_CFG2, max_sqp_iters=1)
+    pr = problem(plant, N, B, seed=17)
+    s = gpu_solver(plant, N, B, precision="fp32", **params)
+    ref = O.Solver(plant, N, B, oracle_params(O, **params), threads=4)
+    xu = pr["xu"].copy()
+    eq = tot = 0
+    errs = []
+    for it in range(5):
+        lam = s.get_lambda()
+        rho = s.get_rho()
+        ref.set_lambda(lam.astype(np.float64))
+        ref.set_rho_penalty_batch(rho.astype(np.float64), False)
+        g = s.solve_raw(xu, 0.01, pr["xs"], pr["goal"])
+        xo, so = ref.solve(xu.astype(np.float64), 0.01, pr["xs"], pr["goal"])
+        pg, po = g["pcg_iters"].ravel(), so["pcg_iters"].ravel()
+        eq += int(np.sum(pg == po))
+        tot += pg.size
+        assert np.all(np.abs(pg - po) <= np.maximum(2, 0.15 * po)), (pg, po)
+        same = g["ls_step_size"].ravel() == so["ls_step_size"].ravel().astype(np.float32)
+        for b in np.nonzero(same)[0]:
+            errs.append(nerr(g["XU"][b], xo[b]))
+        xu = g["XU"]
+    s.close()
+    assert eq >= 0.85 * tot, (eq, tot)
+    assert errs and max(errs) < 5e-3 and float(np.median(errs)) < 1e-3, errs
+
+
+def test_plain_and_fused_forms_are_bitwise_identical():
+    plant, N, B = "iiwa14", 32, 16
+    pr = problem(plant, N, B, seed=23)
+    outs = []
+    for form in ("plain", "fused"):
+        s = gpu_solver(plant, N, B, form=form, **PARAMS_CFG2)
+        outs.append((s.solve_raw(pr["xu"], 0.01, pr["xs"], pr["goal"]), s.get_lambda()))
+        s.close()
+    (a, la), (b, lb) = outs
+    np.testing.assert_array_equal(a["XU"], b["XU"])
+    np.testing.assert_array_equal(la, lb)
+    np.testing.assert_array_equal(a["pcg_iters"], b["pcg_iters"])
+    np.testing.assert_array_equal(a["final_merit"], b["final_merit"])
+
+
+def test_interface_drop_in_surface():
+    """interface.BSQP call pattern of the reference's MPC loop
+    (python/bsqp/mpc_controller.py:235-242): solve, stats, resets, setters."""
+    import gato_b200
+    N, B = 16, 4
+    pr = problem("indy7", N, B, seed=2, perturbed=False)
+    s = gato_b200.BSQP(batch_size=B, N=N, dt=0.01, plant_type="indy7", max_sqp_iters=3,
+                       rho=1e-3)
+    XU, t_us = s.solve(pr["xs"], pr["goal"], pr["xu"])
+    assert XU.shape == (B, s.traj_size) and t_us > 0
+    st = s.get_stats()
+    for k in ["sqp_time_us", "sqp_iters", "kkt_converged", "pcg_iters", "pcg_times_us",
+              "min_merit", "step_size", "initial_merit", "final_merit", "ls_num_iters",
+              "best_merit_per_iter"]:
+        assert k in st, k
+    assert st["pcg_iters"].shape == (st["ls_num_iters"], B)
+    s.set_rho_penalty_batch(np.full(B, 0.05), True)
+    s.reset_rho()
+    np.testing.assert_allclose(s.get_rho(), 0.05, rtol=1e-6)
+    s.reset_dual()
+    assert np.all(s.get_lambda() == 0)
+    s.set_mu_batch(np.full(B, 5.0))
+    s.set_pcg_tol_batch(np.full(B, 1e-4))
+    XU2, _ = s.solve(pr["xs"], pr["goal"])
+    assert np.all(np.isfinite(XU2))
+    assert s.sim_forward(pr["xs"][0], np.zeros(6), 0.01).shape == (B, 12)
+    p = s.ee_pos(pr["xs"][0][:6])
+    assert p.shape == (3,)
+    s.close()
