@@ -435,11 +435,42 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
 {
     constexpr int NQ = Tg::NQ;
     using T = typename Tg::T;
+    using Acc = typename Tg::Acc;
+    if (RowPcg<NQ>::fits(s->N)) {
+        // KKT + Schur into global memory, then the register-resident PCG + dz
+        {
+            ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
+            FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, false};
+            k_fused_iter<NQ, T, Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(bt, dmodel<Tg>(s),
+                                                                              0, row, 0);
+            CKL();
+        }
+        ProfScope ps2_(s, st, GATO_KERNEL_PCG);
+        k_pcg_rows<NQ, T, Acc><<<s->B, RowPcg<NQ>::threads(s->N),
+                                  RowPcg<NQ>::template smem_bytes<T>(s->N), st>>>(bt, row);
+        CKL();
+        return GATO_OK;
+    }
     ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
     const bool stage = fused_stage_fits<Tg>(s);
     FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, stage};
-    k_fused_iter<NQ, T, typename Tg::Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(
-        bt, dmodel<Tg>(s), stage, row);
+    k_fused_iter<NQ, T, Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(bt, dmodel<Tg>(s), stage,
+                                                                      row, 1);
+    CKL();
+    return GATO_OK;
+}
+
+template <class Tg>
+int launch_merit_ls(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt,
+                    int mode, int row)
+{
+    using T = typename Tg::T;
+    using Acc = typename Tg::Acc;
+    ProfScope ps_(s, st, mode == 1 ? GATO_KERNEL_LINE_SEARCH : GATO_KERNEL_MERIT);
+    const int items = (mode == 1 ? NUM_ALPHAS : 1) * s->N;
+    const int threads = std::min(256, cdiv(items, WARP) * WARP);
+    k_merit_ls<Tg::NQ, T, Acc><<<s->B, threads, items * sizeof(Acc), st>>>(bt, dmodel<Tg>(s),
+                                                                           mode, row);
     CKL();
     return GATO_OK;
 }
@@ -465,6 +496,7 @@ int configure_kernels(gato_solver* s)
         return fail(GATO_ERR_UNSUPPORTED, "N=%d needs %zu bytes of shared memory", s->N,
                     lay.bytes());
     RC(set_smem(k_fused_iter<NQ, T, Acc>, lay.bytes()));
+    RC(set_smem(k_pcg_rows<NQ, T, Acc>, RowPcg<NQ>::template smem_bytes<T>(s->N)));
     return GATO_OK;
 }
 
@@ -527,16 +559,13 @@ int enqueue_fused(gato_solver* s, cudaStream_t st, void* xu, const void* xs, con
     CK(cudaMemsetAsync(s->sqp_iters, 0, sizeof(int) * B, st));
     CK(cudaMemsetAsync(s->done, 0, sizeof(int), st));
     CK(cudaMemsetAsync(s->ls_count, 0, sizeof(int), st));
-    RC(launch_merit<Tg>(s, st, bt, 1, 0, 0));
-    RC(launch_merit_sum<Tg>(s, st, s->merit_init, s->merit_init0));
+    RC(launch_merit_ls<Tg>(s, st, bt, 0, 0));
     for (int it = 0; it < s->params.max_sqp_iters; ++it) {
         RC(launch_fused_iter<Tg>(s, st, bt, it));
         RC(launch_check<Tg>(s, st, bt));
-        RC(launch_merit<Tg>(s, st, bt, NUM_ALPHAS, 1, 1));
-        RC(launch_ls<Tg>(s, st, bt, it, 1));
+        RC(launch_merit_ls<Tg>(s, st, bt, 1, it));
     }
-    RC(launch_merit<Tg>(s, st, bt, 1, 0, 0));
-    RC(launch_merit_sum<Tg>(s, st, s->merit_final, nullptr));
+    RC(launch_merit_ls<Tg>(s, st, bt, 2, 0));
     CK(cudaMemcpyAsync(s->drho, s->drho_init_d, s->esz * B, cudaMemcpyDeviceToDevice, st));
     return GATO_OK;
 }

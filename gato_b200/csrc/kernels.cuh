@@ -10,6 +10,7 @@
 
 #include "common.cuh"
 #include "dynamics.cuh"
+#include "dynamics_thread.cuh"
 #include "stages.cuh"
 
 namespace gato {
@@ -138,6 +139,98 @@ __global__ void k_line_search(Batch<NQ, T> bt, int it, int skip_if_done)
         const Dims<NQ> d{N};
         T* x = bt.xu + (size_t)b * d.traj();
         const T* dz = bt.dz + (size_t)b * d.traj();
+        const T st = s_step;
+        for (int i = t; i < d.traj(); i += blockDim.x) x[i] += st * dz[i];
+    }
+}
+
+// ------------------------------------------------------------------ merit + line search
+// One block per problem, one thread per (step size, knot) sample
+// (computeMeritBatchedKernel + lineSearchAndUpdateBatchedKernel,
+// gato/bsqp/kernels/merit.cuh:16-92, line_search.cuh:12-98).  The merit sum of
+// each step size is formed in knot order in Acc precision.
+//   mode 0: merit of XU (alpha = 1, no step)  -> merit_init, merit_init0
+//   mode 1: line search over NUM_ALPHAS steps -> rho, step, XU update
+//   mode 2: merit of XU                       -> merit_final
+template <int NQ, typename T, typename Acc>
+__global__ void __launch_bounds__(256) k_merit_ls(Batch<NQ, T> bt, DevModel<NQ, T> M, int mode,
+                                                  int it)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Acc* terms = reinterpret_cast<Acc*>(smem_raw);
+    __shared__ Acc s_m[NUM_ALPHAS];
+    __shared__ T s_step;
+    __shared__ int s_ok;
+    if (mode == 1 && *bt.done) return;
+    const int b = blockIdx.x;
+    const int N = bt.N;
+    const int nalpha = (mode == 1) ? NUM_ALPHAS : 1;
+    const Dims<NQ> d{N};
+    const T* xu = bt.xu + (size_t)b * d.traj();
+    const T* dz = (mode == 1) ? bt.dz + (size_t)b * d.traj() : nullptr;
+    const T mu = bt.mu[b];
+    const T* fext = bt.use_fext ? bt.fext + 6 * b : nullptr;
+    for (int item = threadIdx.x; item < nalpha * N; item += blockDim.x) {
+        const int k = item % N, j = item / N;
+        const T alpha = T(1) / (T)(1 << j);
+        terms[item] = (Acc)merit_thread<NQ, T>(M, bt.cp, N, k, alpha, mu, xu, dz,
+                                               bt.xs + (size_t)b * Dims<NQ>::nx,
+                                               bt.goal + (size_t)b * d.goal(), fext);
+    }
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < nalpha) {
+        Acc sum = 0;
+        for (int k = 0; k < N; ++k) sum += terms[t * N + k];
+        s_m[t] = sum;
+    }
+    __syncthreads();
+    if (mode != 1) {
+        if (t == 0) {
+            if (mode == 0) {
+                bt.merit_init[b] = (double)s_m[0];
+                bt.merit_init0[b] = (double)s_m[0];
+            } else {
+                bt.merit_final[b] = (double)s_m[0];
+            }
+        }
+        return;
+    }
+    if (t == 0) {
+        Acc best = (Acc)1e38;
+        int bj = 0;
+        for (int j = 0; j < NUM_ALPHAS; ++j)
+            if (s_m[j] < best) {
+                best = s_m[j];
+                bj = j;
+            }
+        const bool ok = best < (Acc)bt.merit_init[b];
+        if (bt.adapt_rho) {
+            const T dr = bt.drho[b];
+            const T fac = T(RHO_FACTOR);
+            const T mult = ok ? gmin(dr / fac, T(1) / fac) : gmax(dr * fac, fac);
+            bt.drho[b] = mult;
+            const T rr = gmax(bt.rho[b] * mult, T(RHO_MIN));
+            bt.rho[b] = gmin(rr, T(RHO_MAX));
+        }
+        T step;
+        if (!ok) {
+            if (bt.rho[b] > T(RHO_MAX)) bt.rho[b] = T(RHO_INIT);
+            step = T(-1);
+        } else {
+            step = T(1) / (T)(1 << bj);
+            bt.merit_init[b] = (double)best;
+        }
+        s_step = step;
+        s_ok = ok;
+        if (bt.h_ls_min) {
+            bt.h_ls_min[(size_t)it * bt.B + b] = (float)bt.merit_init[b];
+            bt.h_ls_step[(size_t)it * bt.B + b] = (float)step;
+        }
+    }
+    __syncthreads();
+    if (s_ok) {
+        T* x = bt.xu + (size_t)b * d.traj();
         const T st = s_step;
         for (int i = t; i < d.traj(); i += blockDim.x) x[i] += st * dz[i];
     }
@@ -389,6 +482,210 @@ __global__ void k_pcg(Batch<NQ, T> bt, int stage, int it_row)
     }
 }
 
+// ------------------------------------------------------------------ row PCG
+// Preconditioned CG with the matrices resident in registers: thread r owns
+// row r of the block-tridiagonal S and P^-1 (3n entries each) and entry r of
+// every CG vector; only p and r go through shared memory, where each thread
+// reads the 3n-wide window of its block row with 16-byte loads.  Vectors use
+// a block stride VS (n rounded up to a multiple of 4) so windows are aligned.
+// Same iteration as pcg_block (gato/bsqp/kernels/pcg.cuh:23-147).  After the
+// solve the block computes the step dz of every knot (dz_knot's algebra).
+template <int NQ>
+struct RowPcg {
+    static constexpr int n = 2 * NQ, m = NQ, RD = 3 * n, VS = (n + 3) & ~3;
+    static constexpr int MAX_THREADS = 512;
+    // rows handled by one block: one per thread
+    __host__ __device__ static int threads(int N) { return ((N * n + 31) / 32) * 32; }
+    __host__ __device__ static bool fits(int N) { return N * n <= MAX_THREADS; }
+    template <typename T>
+    __host__ __device__ static size_t smem_bytes(int N)
+    {
+        return 2 * (size_t)(N + 2) * VS * sizeof(T) + 2 * WARP * sizeof(double) + 16;
+    }
+};
+
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+    static constexpr int W = 4;
+    __device__ static void load(const float* p, float* o)
+    {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    }
+};
+template <>
+struct Vec16<double> {
+    static constexpr int W = 2;
+    __device__ static void load(const double* p, double* o)
+    {
+        const double2 v = *reinterpret_cast<const double2*>(p);
+        o[0] = v.x; o[1] = v.y;
+    }
+};
+
+// row . window over the three blocks of a padded vector, four partial sums
+template <int NQ, typename T>
+__device__ __forceinline__ T row_window_dot(const T (&row)[RowPcg<NQ>::RD], const T* win)
+{
+    constexpr int n = RowPcg<NQ>::n, VS = RowPcg<NQ>::VS, W = Vec16<T>::W;
+    T acc[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+    for (int blk = 0; blk < 3; ++blk) {
+#pragma unroll
+        for (int c0 = 0; c0 < VS; c0 += W) {
+            T v[W];
+            Vec16<T>::load(win + blk * VS + c0, v);
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                const int c = c0 + w;
+                if (c < n) acc[c & 3] += row[blk * n + c] * v[w];
+            }
+        }
+    }
+    return (acc[0] + acc[1]) + (acc[2] + acc[3]);
+}
+
+template <typename Acc>
+__device__ __forceinline__ Acc rows_block_sum(Acc v, Acc* red)
+{
+    v = warp_sum(v);
+    if (lane_id() == 0) red[warp_id()] = v;
+    __syncthreads();
+    Acc s = 0;
+    const int nw = blockDim.x / WARP;
+    for (int w = 0; w < nw; ++w) s += red[w];
+    return s;
+}
+
+template <int NQ, typename T, typename Acc>
+__global__ void __launch_bounds__(RowPcg<NQ>::MAX_THREADS, 1)
+    k_pcg_rows(Batch<NQ, T> bt, int it_row)
+{
+    using RP = RowPcg<NQ>;
+    constexpr int n = RP::n, m = RP::m, RD = RP::RD, VS = RP::VS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (*bt.done) return;
+    const int b = blockIdx.x;
+    const int N = bt.N;
+    const Dims<NQ> d{N};
+    const int tid = threadIdx.x;
+    const bool act = tid < N * n;
+    const int k = act ? tid / n : 0, i = act ? tid % n : 0;
+    const int L = (N + 2) * VS;
+    T* pv = reinterpret_cast<T*>(smem_raw);
+    T* rv = pv + L;
+    Acc* red = reinterpret_cast<Acc*>(((uintptr_t)(rv + L) + 15) & ~(uintptr_t)15);
+    for (int j = tid; j < 2 * L; j += blockDim.x) pv[j] = T(0);
+    T* lam = bt.lambda + (size_t)b * d.vecp();
+    const int own = (k + 1) * VS + i;
+    const T* winp = pv + k * VS;
+    const T* winr = rv + k * VS;
+    int iters = 0;
+    T x = act ? lam[(k + 1) * n + i] : T(0);
+    if (!bt.conv[b]) {
+        T srow[RD], prow[RD];
+        const T* Sg = bt.S + (size_t)b * d.b3d() + (size_t)(k * n + i) * RD;
+        const T* Pg = bt.P + (size_t)b * d.b3d() + (size_t)(k * n + i) * RD;
+#pragma unroll
+        for (int c = 0; c < RD; ++c) {
+            srow[c] = act ? Sg[c] : T(0);
+            prow[c] = act ? Pg[c] : T(0);
+        }
+        const T g = act ? bt.gamma[(size_t)b * d.vecp() + (k + 1) * n + i] : T(0);
+        __syncthreads();
+        if (act) pv[own] = x;
+        __syncthreads();
+        T r = act ? g - row_window_dot<NQ, T>(srow, winp) : T(0);
+        if (act) rv[own] = r;
+        __syncthreads();
+        T z = row_window_dot<NQ, T>(prow, winr);
+        Acc rho = rows_block_sum<Acc>(act ? (Acc)r * (Acc)z : Acc(0), red);
+        T p = z;
+        const Acc abs_tol = Acc(1e-6);
+        const T eps = bt.tol[b];
+        if (!(fabs((double)rho) < (double)abs_tol)) {
+            const Acc rho_init = rho < 0 ? -rho : rho;
+            for (int it = 0; it < bt.max_pcg_iters; ++it) {
+                ++iters;
+                if (act) pv[own] = p;
+                __syncthreads();
+                const T ap = row_window_dot<NQ, T>(srow, winp);
+                const Acc pap = rows_block_sum<Acc>(act ? (Acc)p * (Acc)ap : Acc(0), red);
+                const T alpha = (T)(rho / pap);
+                x += alpha * p;
+                r -= alpha * ap;
+                if (act) rv[own] = r;
+                __syncthreads();
+                z = row_window_dot<NQ, T>(prow, winr);
+                const Acc rho_new = rows_block_sum<Acc>(act ? (Acc)r * (Acc)z : Acc(0), red + WARP);
+                const Acc arn = rho_new < 0 ? -rho_new : rho_new;
+                if (arn < abs_tol + (Acc)eps * rho_init) break;
+                const T beta = (T)(rho_new / rho);
+                rho = rho_new;
+                p = z + beta * p;
+            }
+            if (act) lam[(k + 1) * n + i] = x;
+        }
+    }
+    // step recovery (computeDzBatchedKernel, schur_linsys.cuh:312-431):
+    // res_x = q_k - lambda_k + A_k^T lambda_{k+1}, dz_x = -Qi_k res_x,
+    // res_u = r_k + B_k^T lambda_{k+1}, dz_u = -Ri_k res_u
+    __syncthreads();
+    if (act) pv[own] = x;
+    __syncthreads();
+    const T* lk1 = pv + (k + 2) * VS;
+    T res = T(0), resu = T(0);
+    if (act) {
+        const T* A = bt.A + ((size_t)b * N + k) * n * n;
+        T acc = T(0);
+        if (k < N - 1) {
+#pragma unroll
+            for (int t = 0; t < n; ++t) acc += lk1[t] * A[i * n + t];
+        }
+        res = bt.q[((size_t)b * N + k) * n + i] - x + acc;
+        bt.q[((size_t)b * N + k) * n + i] = res;
+        if (i < m) {
+            if (k < N - 1) {
+                const T* Bm = bt.Bm + ((size_t)b * N + k) * n * m;
+                T accu = T(0);
+#pragma unroll
+                for (int t = 0; t < n; ++t) accu += lk1[t] * Bm[i * n + t];
+                resu = bt.r[((size_t)b * N + k) * m + i] + accu;
+            }
+            bt.r[((size_t)b * N + k) * m + i] = resu;
+        }
+    }
+    __syncthreads();
+    if (act) {
+        rv[own] = res;
+        if (i < m) pv[k * m + i] = resu;  // lambda is no longer read
+    }
+    __syncthreads();
+    if (act) {
+        const T* Qi = bt.Qi + ((size_t)b * N + k) * n * n;
+        const T* rk = rv + (k + 1) * VS;
+        T acc = T(0);
+#pragma unroll
+        for (int t = 0; t < n; ++t) acc += Qi[t * n + i] * rk[t];
+        T* dzk = bt.dz + (size_t)b * d.traj() + k * (n + m);
+        dzk[i] = -acc;
+        if (i < m && k < N - 1) {
+            const T* Ri = bt.Ri + ((size_t)b * N + k) * m * m;
+            const T* ru = pv + k * m;
+            T accu = T(0);
+#pragma unroll
+            for (int t = 0; t < m; ++t) accu += Ri[t * m + i] * ru[t];
+            dzk[n + i] = -accu;
+        }
+    }
+    if (tid == 0) {
+        bt.pcg_iters[b] = iters;
+        if (bt.h_pcg) bt.h_pcg[(size_t)it_row * bt.B + b] = iters;
+    }
+}
+
 // ------------------------------------------------------------------ dz
 template <int NQ, typename T>
 __global__ void k_dz(Batch<NQ, T> bt)
@@ -473,9 +770,12 @@ struct FusedLayout {
 };
 
 // One SQP iteration of one problem up to the step (KKT set-up, Schur
-// complement, PCG, step recovery), one block.
+// complement, PCG, step recovery), one block.  With with_pcg = 0 it stops
+// after the Schur complement (S, P^-1 and gamma left in global memory) and
+// k_pcg_rows takes over.
 template <int NQ, typename T, typename Acc>
-__global__ void k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int it_row)
+__global__ void k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int it_row,
+                             int with_pcg)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
@@ -539,6 +839,7 @@ __global__ void k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int 
     }
     __syncthreads();
     for (int k = warp_id(); k < N - 1; k += nw) schur_offdiag<NQ, T>(k, S, P, ws);
+    if (!with_pcg) return;  // k_pcg_rows continues from S, P^-1 in global memory
     __syncthreads();
     int iters = 0;
     if (!bt.conv[b])
