@@ -436,7 +436,10 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
     constexpr int NQ = Tg::NQ;
     using T = typename Tg::T;
     using Acc = typename Tg::Acc;
-    if (RowPcg<NQ>::fits(s->N)) {
+    // rows of S and P^-1 per thread in k_pcg_rows: two in FP32 (each window
+    // value loaded from shared memory feeds two rows), one in FP64 (registers)
+    constexpr int RPT = sizeof(T) == 4 ? 2 : 1;
+    if (RowPcg<NQ, RPT>::fits(s->N)) {
         // KKT + Schur into global memory, then the register-resident PCG + dz
         {
             ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
@@ -446,8 +449,9 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
             CKL();
         }
         ProfScope ps2_(s, st, GATO_KERNEL_PCG);
-        k_pcg_rows<NQ, T, Acc><<<s->B, RowPcg<NQ>::threads(s->N),
-                                  RowPcg<NQ>::template smem_bytes<T>(s->N), st>>>(bt, row);
+        k_pcg_rows<NQ, T, Acc, RPT><<<s->B, RowPcg<NQ, RPT>::threads(s->N),
+                                       RowPcg<NQ, RPT>::template smem_bytes<T>(s->N), st>>>(bt,
+                                                                                            row);
         CKL();
         return GATO_OK;
     }
@@ -496,7 +500,8 @@ int configure_kernels(gato_solver* s)
         return fail(GATO_ERR_UNSUPPORTED, "N=%d needs %zu bytes of shared memory", s->N,
                     lay.bytes());
     RC(set_smem(k_fused_iter<NQ, T, Acc>, lay.bytes()));
-    RC(set_smem(k_pcg_rows<NQ, T, Acc>, RowPcg<NQ>::template smem_bytes<T>(s->N)));
+    constexpr int RPT = sizeof(T) == 4 ? 2 : 1;
+    RC(set_smem(k_pcg_rows<NQ, T, Acc, RPT>, RowPcg<NQ, RPT>::template smem_bytes<T>(s->N)));
     return GATO_OK;
 }
 

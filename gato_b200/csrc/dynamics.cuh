@@ -95,10 +95,10 @@ __device__ __forceinline__ void i_mul(const DevModel<NQ, T>& M, int i, const T* 
 // ---------------------------------------------------------------------------
 // per-knot set-up: sin/cos and the joint transforms X_i(q_i) into scratch.
 // Must be followed by __syncwarp() before use.
-template <int NQ, typename T>
+template <int NQ, typename T, int G = 32>
 __device__ __forceinline__ void dyn_load_transforms(const DevModel<NQ, T>& M, const T* q, T* s)
 {
-    const int l = lane_id();
+    const int l = lane_id() & (G - 1);
     if (l < NQ) {
         T sn, cs;
         gsincos(q[l], &sn, &cs);
@@ -173,14 +173,15 @@ __device__ __forceinline__ void rnea_lane(const DevModel<NQ, T>& M, const T* s, 
 // In-place pivot-free Gauss-Jordan across lanes: lane c holds column c of an
 // augmented [A | I] (DIM rows); lanes DIM..2DIM-1 end with the columns of
 // A^-1.  Follows the elimination order of gato/utils/linalg.cuh:364-400.
-template <int DIM, typename T>
+// G is the lane-group width (16: two independent systems per warp).
+template <int DIM, typename T, int G = 32>
 __device__ __forceinline__ void warp_gj(T (&col)[DIM])
 {
 #pragma unroll
     for (int k = 0; k < DIM; ++k) {
         T pk[DIM];
 #pragma unroll
-        for (int r = 0; r < DIM; ++r) pk[r] = __shfl_sync(FULL, col[r], k);
+        for (int r = 0; r < DIM; ++r) pk[r] = __shfl_sync(FULL, col[r], k, G);
         const T rcp = T(1.0) / pk[k];
         const T rowk = col[k];
 #pragma unroll
@@ -193,12 +194,13 @@ __device__ __forceinline__ void warp_gj(T (&col)[DIM])
 // Forward dynamics of one knot: qdd into scratch (QDD) and, when with_minv,
 // M^-1 column-major into scratch (MINV).  Needs dyn_load_transforms first.
 // Returns, in lanes NQ..2NQ-1, column (lane-NQ) of M^-1 in minv_col.
-template <int NQ, typename T>
+template <int NQ, typename T, int G = 32>
 __device__ __forceinline__ void dyn_forward(const DevModel<NQ, T>& M, T* s, const T* q,
                                             const T* qd, const T* u, const T* fext,
                                             bool with_minv, T (&minv_col)[NQ])
 {
-    const int l = lane_id();
+    static_assert(2 * NQ < G, "the bias lane must lie inside the lane group");
+    const int l = lane_id() & (G - 1);
     const bool bias = (l == 2 * NQ);
     T tau[NQ];
     rnea_lane<NQ, T>(M, s, qd, bias ? T(1.0) : T(0.0), (l < NQ) ? l : -1, bias ? M.gravity : T(0.0),
@@ -207,12 +209,12 @@ __device__ __forceinline__ void dyn_forward(const DevModel<NQ, T>& M, T* s, cons
     T col[NQ];
 #pragma unroll
     for (int r = 0; r < NQ; ++r) col[r] = (l < NQ) ? tau[r] : ((l - NQ == r) ? T(1.0) : T(0.0));
-    warp_gj<NQ, T>(col);
+    warp_gj<NQ, T, G>(col);
     // bias c from lane 2NQ; qdd_r = (M^-1 column r) . (u - c)  (M^-1 symmetric)
     T qdd = T(0.0);
 #pragma unroll
     for (int r = 0; r < NQ; ++r) {
-        const T cr = __shfl_sync(FULL, tau[r], 2 * NQ);
+        const T cr = __shfl_sync(FULL, tau[r], 2 * NQ, G);
         qdd += col[r] * (u[r] - cr);
     }
     if (l >= NQ && l < 2 * NQ) {
@@ -229,12 +231,12 @@ __device__ __forceinline__ void dyn_forward(const DevModel<NQ, T>& M, T* s, cons
 
 // Forward-mode derivative of the RNEA recursions at (q, qd, qdd) with f_ext:
 // lane j < 2NQ returns column j of [dtau/dq | dtau/dqd] in dtau.
-template <int NQ, typename T>
+template <int NQ, typename T, int G = 32>
 __device__ __forceinline__ void rnea_derivative_lane(const DevModel<NQ, T>& M, const T* s,
                                                      const T* qd, const T* qdd,
                                                      const T* fext, T* dtau)
 {
-    const int l = lane_id();
+    const int l = lane_id() & (G - 1);
     const bool wq = l < NQ;
     const int j = wq ? l : l - NQ;
     T v[6] = {0, 0, 0, 0, 0, 0};
@@ -315,10 +317,10 @@ __device__ __forceinline__ void rnea_derivative_lane(const DevModel<NQ, T>& M, c
 // iiwa14_grid.cuh:2596-2672) computed redundantly by every lane; lane j < NQ
 // also gets the position Jacobian column dp/dq_j = z_j x (p - o_j)
 // (iiwa14_grid.cuh:2855-2966).  Needs dyn_load_transforms (sin/cos).
-template <int NQ, typename T>
+template <int NQ, typename T, int G = 32>
 __device__ __forceinline__ void fk_lane(const DevModel<NQ, T>& M, const T* s, T* p, T* J)
 {
-    const int l = lane_id();
+    const int l = lane_id() & (G - 1);
     T R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     T o[3] = {0, 0, 0};
     T zj[3] = {0, 0, 0}, oj[3] = {0, 0, 0};

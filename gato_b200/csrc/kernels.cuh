@@ -483,20 +483,22 @@ __global__ void k_pcg(Batch<NQ, T> bt, int stage, int it_row)
 }
 
 // ------------------------------------------------------------------ row PCG
-// Preconditioned CG with the matrices resident in registers: thread r owns
-// row r of the block-tridiagonal S and P^-1 (3n entries each) and entry r of
-// every CG vector; only p and r go through shared memory, where each thread
-// reads the 3n-wide window of its block row with 16-byte loads.  Vectors use
-// a block stride VS (n rounded up to a multiple of 4) so windows are aligned.
-// Same iteration as pcg_block (gato/bsqp/kernels/pcg.cuh:23-147).  After the
-// solve the block computes the step dz of every knot (dz_knot's algebra).
-template <int NQ>
+// Preconditioned CG with the matrices resident in registers: each thread owns
+// RPT rows of one block row of S and P^-1 (3n entries per row) and the
+// matching entries of every CG vector; only p and r go through shared memory,
+// where a thread reads the 3n-wide window of its block row once with 16-byte
+// loads and applies it to all of its rows.  Vectors use a block stride VS (n
+// rounded up to a multiple of 4) so windows are aligned.  Same iteration as
+// pcg_block (gato/bsqp/kernels/pcg.cuh:23-147).  After the solve the block
+// computes the step dz of every knot (dz_knot's algebra).
+template <int NQ, int RPT>
 struct RowPcg {
     static constexpr int n = 2 * NQ, m = NQ, RD = 3 * n, VS = (n + 3) & ~3;
-    static constexpr int MAX_THREADS = 512;
-    // rows handled by one block: one per thread
-    __host__ __device__ static int threads(int N) { return ((N * n + 31) / 32) * 32; }
-    __host__ __device__ static bool fits(int N) { return N * n <= MAX_THREADS; }
+    static constexpr int TPB = n / RPT;  // threads per block row
+    static_assert(n % RPT == 0, "rows per thread must divide n");
+    static constexpr int MAX_THREADS = 512 / RPT;
+    __host__ __device__ static int threads(int N) { return ((N * TPB + 31) / 32) * 32; }
+    __host__ __device__ static bool fits(int N) { return N * TPB <= MAX_THREADS; }
     template <typename T>
     __host__ __device__ static size_t smem_bytes(int N)
     {
@@ -525,12 +527,18 @@ struct Vec16<double> {
     }
 };
 
-// row . window over the three blocks of a padded vector, four partial sums
-template <int NQ, typename T>
-__device__ __forceinline__ T row_window_dot(const T (&row)[RowPcg<NQ>::RD], const T* win)
+// out[j] = row[j] . window for the RPT rows of a thread (three blocks of a
+// padded vector, four partial sums per row)
+template <int NQ, int RPT, typename T>
+__device__ __forceinline__ void rows_window_dot(const T (&row)[RPT][3 * 2 * NQ], const T* win,
+                                                T (&out)[RPT])
 {
-    constexpr int n = RowPcg<NQ>::n, VS = RowPcg<NQ>::VS, W = Vec16<T>::W;
-    T acc[4] = {T(0), T(0), T(0), T(0)};
+    constexpr int n = 2 * NQ, VS = (n + 3) & ~3, W = Vec16<T>::W;
+    T acc[RPT][4];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j)
+#pragma unroll
+        for (int a = 0; a < 4; ++a) acc[j][a] = T(0);
 #pragma unroll
     for (int blk = 0; blk < 3; ++blk) {
 #pragma unroll
@@ -540,11 +548,15 @@ __device__ __forceinline__ T row_window_dot(const T (&row)[RowPcg<NQ>::RD], cons
 #pragma unroll
             for (int w = 0; w < W; ++w) {
                 const int c = c0 + w;
-                if (c < n) acc[c & 3] += row[blk * n + c] * v[w];
+                if (c < n) {
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) acc[j][c & 3] += row[j][blk * n + c] * v[w];
+                }
             }
         }
     }
-    return (acc[0] + acc[1]) + (acc[2] + acc[3]);
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) out[j] = (acc[j][0] + acc[j][1]) + (acc[j][2] + acc[j][3]);
 }
 
 template <typename Acc>
@@ -559,125 +571,177 @@ __device__ __forceinline__ Acc rows_block_sum(Acc v, Acc* red)
     return s;
 }
 
-template <int NQ, typename T, typename Acc>
-__global__ void __launch_bounds__(RowPcg<NQ>::MAX_THREADS, 1)
+template <int NQ, typename T, typename Acc, int RPT>
+__global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
     k_pcg_rows(Batch<NQ, T> bt, int it_row)
 {
-    using RP = RowPcg<NQ>;
-    constexpr int n = RP::n, m = RP::m, RD = RP::RD, VS = RP::VS;
+    using RP = RowPcg<NQ, RPT>;
+    constexpr int n = RP::n, m = RP::m, RD = RP::RD, VS = RP::VS, TPB = RP::TPB;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (*bt.done) return;
     const int b = blockIdx.x;
     const int N = bt.N;
     const Dims<NQ> d{N};
     const int tid = threadIdx.x;
-    const bool act = tid < N * n;
-    const int k = act ? tid / n : 0, i = act ? tid % n : 0;
+    const bool act = tid < N * TPB;
+    const int k = act ? tid / TPB : 0, i0 = act ? tid % TPB : 0;
     const int L = (N + 2) * VS;
     T* pv = reinterpret_cast<T*>(smem_raw);
     T* rv = pv + L;
     Acc* red = reinterpret_cast<Acc*>(((uintptr_t)(rv + L) + 15) & ~(uintptr_t)15);
     for (int j = tid; j < 2 * L; j += blockDim.x) pv[j] = T(0);
     T* lam = bt.lambda + (size_t)b * d.vecp();
-    const int own = (k + 1) * VS + i;
-    const T* winp = pv + k * VS;
-    const T* winr = rv + k * VS;
+    const int w0 = k * VS;
     int iters = 0;
-    T x = act ? lam[(k + 1) * n + i] : T(0);
-    if (!bt.conv[b]) {
-        T srow[RD], prow[RD];
-        const T* Sg = bt.S + (size_t)b * d.b3d() + (size_t)(k * n + i) * RD;
-        const T* Pg = bt.P + (size_t)b * d.b3d() + (size_t)(k * n + i) * RD;
+    T x[RPT];
 #pragma unroll
-        for (int c = 0; c < RD; ++c) {
-            srow[c] = act ? Sg[c] : T(0);
-            prow[c] = act ? Pg[c] : T(0);
+    for (int j = 0; j < RPT; ++j) x[j] = act ? lam[(k + 1) * n + i0 + j * TPB] : T(0);
+    if (!bt.conv[b]) {
+        T srow[RPT][RD], prow[RPT][RD];
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+            const size_t row = (size_t)(k * n + i0 + j * TPB) * RD;
+            const T* Sg = bt.S + (size_t)b * d.b3d() + row;
+            const T* Pg = bt.P + (size_t)b * d.b3d() + row;
+#pragma unroll
+            for (int c = 0; c < RD; ++c) {
+                srow[j][c] = act ? Sg[c] : T(0);
+                prow[j][c] = act ? Pg[c] : T(0);
+            }
         }
-        const T g = act ? bt.gamma[(size_t)b * d.vecp() + (k + 1) * n + i] : T(0);
+        T g[RPT], r[RPT], z[RPT], p[RPT], ap[RPT];
+#pragma unroll
+        for (int j = 0; j < RPT; ++j)
+            g[j] = act ? bt.gamma[(size_t)b * d.vecp() + (k + 1) * n + i0 + j * TPB] : T(0);
         __syncthreads();
-        if (act) pv[own] = x;
+        if (act) {
+#pragma unroll
+            for (int j = 0; j < RPT; ++j) pv[(k + 1) * VS + i0 + j * TPB] = x[j];
+        }
         __syncthreads();
-        T r = act ? g - row_window_dot<NQ, T>(srow, winp) : T(0);
-        if (act) rv[own] = r;
+        rows_window_dot<NQ, RPT, T>(srow, pv + w0, r);
+        Acc part = 0;
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+            r[j] = act ? g[j] - r[j] : T(0);
+            if (act) rv[(k + 1) * VS + i0 + j * TPB] = r[j];
+        }
         __syncthreads();
-        T z = row_window_dot<NQ, T>(prow, winr);
-        Acc rho = rows_block_sum<Acc>(act ? (Acc)r * (Acc)z : Acc(0), red);
-        T p = z;
+        rows_window_dot<NQ, RPT, T>(prow, rv + w0, z);
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+            p[j] = z[j];
+            part += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);
+        }
+        Acc rho = rows_block_sum<Acc>(part, red);
         const Acc abs_tol = Acc(1e-6);
         const T eps = bt.tol[b];
         if (!(fabs((double)rho) < (double)abs_tol)) {
             const Acc rho_init = rho < 0 ? -rho : rho;
             for (int it = 0; it < bt.max_pcg_iters; ++it) {
                 ++iters;
-                if (act) pv[own] = p;
+                if (act) {
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) pv[(k + 1) * VS + i0 + j * TPB] = p[j];
+                }
                 __syncthreads();
-                const T ap = row_window_dot<NQ, T>(srow, winp);
-                const Acc pap = rows_block_sum<Acc>(act ? (Acc)p * (Acc)ap : Acc(0), red);
+                rows_window_dot<NQ, RPT, T>(srow, pv + w0, ap);
+                part = 0;
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) part += act ? (Acc)p[j] * (Acc)ap[j] : Acc(0);
+                const Acc pap = rows_block_sum<Acc>(part, red);
                 const T alpha = (T)(rho / pap);
-                x += alpha * p;
-                r -= alpha * ap;
-                if (act) rv[own] = r;
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) {
+                    x[j] += alpha * p[j];
+                    r[j] -= alpha * ap[j];
+                    if (act) rv[(k + 1) * VS + i0 + j * TPB] = r[j];
+                }
                 __syncthreads();
-                z = row_window_dot<NQ, T>(prow, winr);
-                const Acc rho_new = rows_block_sum<Acc>(act ? (Acc)r * (Acc)z : Acc(0), red + WARP);
+                rows_window_dot<NQ, RPT, T>(prow, rv + w0, z);
+                part = 0;
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) part += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);
+                const Acc rho_new = rows_block_sum<Acc>(part, red + WARP);
                 const Acc arn = rho_new < 0 ? -rho_new : rho_new;
                 if (arn < abs_tol + (Acc)eps * rho_init) break;
                 const T beta = (T)(rho_new / rho);
                 rho = rho_new;
-                p = z + beta * p;
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) p[j] = z[j] + beta * p[j];
             }
-            if (act) lam[(k + 1) * n + i] = x;
+            if (act) {
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) lam[(k + 1) * n + i0 + j * TPB] = x[j];
+            }
         }
     }
     // step recovery (computeDzBatchedKernel, schur_linsys.cuh:312-431):
     // res_x = q_k - lambda_k + A_k^T lambda_{k+1}, dz_x = -Qi_k res_x,
     // res_u = r_k + B_k^T lambda_{k+1}, dz_u = -Ri_k res_u
     __syncthreads();
-    if (act) pv[own] = x;
+    if (act) {
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) pv[(k + 1) * VS + i0 + j * TPB] = x[j];
+    }
     __syncthreads();
     const T* lk1 = pv + (k + 2) * VS;
-    T res = T(0), resu = T(0);
-    if (act) {
-        const T* A = bt.A + ((size_t)b * N + k) * n * n;
-        T acc = T(0);
-        if (k < N - 1) {
+    T res[RPT], resu[RPT];
 #pragma unroll
-            for (int t = 0; t < n; ++t) acc += lk1[t] * A[i * n + t];
-        }
-        res = bt.q[((size_t)b * N + k) * n + i] - x + acc;
-        bt.q[((size_t)b * N + k) * n + i] = res;
-        if (i < m) {
+    for (int j = 0; j < RPT; ++j) {
+        res[j] = T(0);
+        resu[j] = T(0);
+        const int i = i0 + j * TPB;
+        if (act) {
+            const T* A = bt.A + ((size_t)b * N + k) * n * n;
+            T acc = T(0);
             if (k < N - 1) {
-                const T* Bm = bt.Bm + ((size_t)b * N + k) * n * m;
+#pragma unroll
+                for (int t = 0; t < n; ++t) acc += lk1[t] * A[i * n + t];
+            }
+            res[j] = bt.q[((size_t)b * N + k) * n + i] - x[j] + acc;
+            bt.q[((size_t)b * N + k) * n + i] = res[j];
+            if (i < m) {
+                if (k < N - 1) {
+                    const T* Bm = bt.Bm + ((size_t)b * N + k) * n * m;
+                    T accu = T(0);
+#pragma unroll
+                    for (int t = 0; t < n; ++t) accu += lk1[t] * Bm[i * n + t];
+                    resu[j] = bt.r[((size_t)b * N + k) * m + i] + accu;
+                }
+                bt.r[((size_t)b * N + k) * m + i] = resu[j];
+            }
+        }
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+            const int i = i0 + j * TPB;
+            rv[(k + 1) * VS + i] = res[j];
+            if (i < m) pv[k * m + i] = resu[j];  // lambda is no longer read
+        }
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+            const int i = i0 + j * TPB;
+            const T* Qi = bt.Qi + ((size_t)b * N + k) * n * n;
+            const T* rk = rv + (k + 1) * VS;
+            T acc = T(0);
+#pragma unroll
+            for (int t = 0; t < n; ++t) acc += Qi[t * n + i] * rk[t];
+            T* dzk = bt.dz + (size_t)b * d.traj() + k * (n + m);
+            dzk[i] = -acc;
+            if (i < m && k < N - 1) {
+                const T* Ri = bt.Ri + ((size_t)b * N + k) * m * m;
+                const T* ru = pv + k * m;
                 T accu = T(0);
 #pragma unroll
-                for (int t = 0; t < n; ++t) accu += lk1[t] * Bm[i * n + t];
-                resu = bt.r[((size_t)b * N + k) * m + i] + accu;
+                for (int t = 0; t < m; ++t) accu += Ri[t * m + i] * ru[t];
+                dzk[n + i] = -accu;
             }
-            bt.r[((size_t)b * N + k) * m + i] = resu;
-        }
-    }
-    __syncthreads();
-    if (act) {
-        rv[own] = res;
-        if (i < m) pv[k * m + i] = resu;  // lambda is no longer read
-    }
-    __syncthreads();
-    if (act) {
-        const T* Qi = bt.Qi + ((size_t)b * N + k) * n * n;
-        const T* rk = rv + (k + 1) * VS;
-        T acc = T(0);
-#pragma unroll
-        for (int t = 0; t < n; ++t) acc += Qi[t * n + i] * rk[t];
-        T* dzk = bt.dz + (size_t)b * d.traj() + k * (n + m);
-        dzk[i] = -acc;
-        if (i < m && k < N - 1) {
-            const T* Ri = bt.Ri + ((size_t)b * N + k) * m * m;
-            const T* ru = pv + k * m;
-            T accu = T(0);
-#pragma unroll
-            for (int t = 0; t < m; ++t) accu += Ri[t * m + i] * ru[t];
-            dzk[n + i] = -accu;
         }
     }
     if (tid == 0) {
@@ -746,7 +810,7 @@ struct FusedLayout {
     bool stage;  // S and P^-1 resident in shared memory
     __host__ __device__ size_t scratch_floats() const
     {
-        int a = KktSmem<NQ>::SIZE, bsz = SchurSmem<NQ>::SIZE, c = 4 * (2 * NQ) * (2 * NQ);
+        int a = 2 * KktSmem<NQ>::SIZE, bsz = SchurSmem<NQ>::SIZE, c = 4 * (2 * NQ) * (2 * NQ);
         int m = a > bsz ? a : bsz;
         m = m > c ? m : c;
         return (size_t)warps * m;
@@ -809,9 +873,18 @@ __global__ void k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int 
     const T* xu = bt.xu + (size_t)b * d.traj();
     const T* fext = bt.use_fext ? bt.fext + 6 * b : nullptr;
 
-    for (int k = warp_id(); k < N - 1; k += nw)
-        kkt_knot<NQ, T>(M, bt.cp, N, k, xu, bt.xs + (size_t)b * nx, bt.goal + (size_t)b * d.goal(),
-                     fext, Q, R, qv, rv, A, Bm, c, ws);
+    // KKT set-up, two knots per warp (one per half-warp)
+    {
+        const int half = lane_id() >> 4;
+        const int npairs = N / 2;  // ceil((N - 1) / 2)
+        for (int kp = warp_id(); kp < npairs; kp += nw) {
+            const int k = 2 * kp + half;
+            const bool valid = k < N - 1;
+            kkt_knot<NQ, T, 16>(M, bt.cp, N, valid ? k : N - 2, xu, bt.xs + (size_t)b * nx,
+                                bt.goal + (size_t)b * d.goal(), fext, Q, R, qv, rv, A, Bm, c,
+                                ws + half * KktSmem<NQ>::SIZE, valid);
+        }
+    }
     __syncthreads();
     for (int k = warp_id(); k < N; k += nw) {
         warp_invert<nx, T>(Q + k * nx * nx, rho, Qi + k * nx * nx);

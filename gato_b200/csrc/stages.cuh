@@ -24,34 +24,37 @@ struct KktSmem {
     static constexpr int SIZE = G + 2 * NQ;
 };
 
-template <int NQ, typename T>
+// G = 16 runs two knots per warp, one per half-warp (all lanes of the warp
+// must call together); `valid` = false evaluates without writing.
+template <int NQ, typename T, int G = 32>
 __device__ void kkt_knot(const DevModel<NQ, T>& M, const CostParams<T>& cp, int N, int k,
                          const T* __restrict__ xu, const T* __restrict__ xs,
                          const T* __restrict__ goal, const T* fext, T* __restrict__ Q,
                          T* __restrict__ R, T* __restrict__ qv, T* __restrict__ rv,
                          T* __restrict__ A, T* __restrict__ Bm, T* __restrict__ c,
-                         T* s)
+                         T* s, bool valid = true)
 {
     using D = Dims<NQ>;
     constexpr int nx = D::nx, nu = D::nu;
-    const int l = lane_id();
+    const int l = valid ? (lane_id() & (G - 1)) : (lane_id() & (G - 1)) + G * 64;
+    const int lg = lane_id() & (G - 1);
     const T* xuk = xu + k * D::nxu;
     T* sx = s + KktSmem<NQ>::XU;
-    for (int i = l; i < 2 * nx + nu; i += WARP) sx[i] = xuk[i];
+    for (int i = lg; i < 2 * nx + nu; i += G) sx[i] = xuk[i];
     __syncwarp();
     const T* q = sx;
     const T* qd = sx + NQ;
     const T* u = sx + nx;
     const T* xk1 = sx + nx + nu;
-    dyn_load_transforms<NQ, T>(M, q, s);
+    dyn_load_transforms<NQ, T, G>(M, q, s);
     __syncwarp();
     T minv_col[NQ];
-    dyn_forward<NQ, T>(M, s, q, qd, u, fext, true, minv_col);
+    dyn_forward<NQ, T, G>(M, s, q, qd, u, fext, true, minv_col);
     T qdd[NQ];
 #pragma unroll
     for (int i = 0; i < NQ; ++i) qdd[i] = s[DynSmem<NQ>::QDD + i];
     T dtau[NQ];
-    rnea_derivative_lane<NQ, T>(M, s, qd, qdd, fext, dtau);
+    rnea_derivative_lane<NQ, T, G>(M, s, qd, qdd, fext, dtau);
     const T dt = cp.dt;
     const T h2 = T(0.5) * dt * dt;
     // integrator_gradient_inner, trapezoidal (integrator.cuh:143-184)
@@ -92,7 +95,7 @@ __device__ void kkt_knot(const DevModel<NQ, T>& M, const CostParams<T>& cp, int 
     // tracking cost gradient and Hessian (iiwa14_plant.cuh:338-424,
     // indy7_plant.cuh:325-420); the weight is q_cost at every KKT knot
     T p[3], J[3];
-    fk_lane<NQ, T>(M, s, p, J);
+    fk_lane<NQ, T, G>(M, s, p, J);
     const T w = cp.q_cost;
     T* sg = s + KktSmem<NQ>::G;
     const int style = M.barrier_style;
@@ -100,9 +103,9 @@ __device__ void kkt_knot(const DevModel<NQ, T>& M, const CostParams<T>& cp, int 
     for (int pass = 0; pass < ((k == N - 2) ? 2 : 1); ++pass) {
         const T* gg = gk + 6 * pass;
         const T e0 = p[0] - gg[0], e1 = p[1] - gg[1], e2 = p[2] - gg[2];
-        if (l < NQ) {
-            sg[l] = J[0] * e0 + J[1] * e1 + J[2] * e2;
-            sg[NQ + l] = barrier_grad(style, q[l], M.qlo[l], M.qhi[l]);
+        if (lg < NQ) {
+            sg[lg] = J[0] * e0 + J[1] * e1 + J[2] * e2;
+            sg[NQ + lg] = barrier_grad(style, q[lg], M.qlo[lg], M.qhi[lg]);
         }
         __syncwarp();
         const int kk = k + pass;
