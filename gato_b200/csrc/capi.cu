@@ -133,11 +133,19 @@ void build_dev_model(const gato_model_t& m, DevModel<NQ, T>* out)
     out->barrier_style = m.barrier_style;
 }
 
+// The dynamic shared-memory limit is a per-kernel attribute shared by every
+// solver on the device, so it is always raised to the device's opt-in
+// maximum: a solver with a small N must not lower it below what a solver
+// with a larger N already relies on.
 template <class K>
-int set_smem(K kernel, size_t bytes)
+int set_smem(K kernel, size_t bytes, int device_limit)
 {
+    if (bytes > (size_t)device_limit)
+        return fail(GATO_ERR_UNSUPPORTED, "kernel needs %zu bytes of shared memory, device has %d",
+                    bytes, device_limit);
     if (bytes > 48 * 1024)
-        CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                device_limit));
     return GATO_OK;
 }
 
@@ -494,14 +502,16 @@ int configure_kernels(gato_solver* s)
     constexpr int NQ = Tg::NQ;
     using T = typename Tg::T;
     using Acc = typename Tg::Acc;
-    RC(set_smem(k_pcg<NQ, T, Acc>, pcg_smem_bytes<NQ, T>(s->N, pcg_stage_fits<Tg>(s))));
+    RC(set_smem(k_pcg<NQ, T, Acc>, pcg_smem_bytes<NQ, T>(s->N, pcg_stage_fits<Tg>(s)),
+                s->max_smem));
     FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, fused_stage_fits<Tg>(s)};
     if (lay.bytes() > (size_t)s->max_smem)
         return fail(GATO_ERR_UNSUPPORTED, "N=%d needs %zu bytes of shared memory", s->N,
                     lay.bytes());
-    RC(set_smem(k_fused_iter<NQ, T, Acc>, lay.bytes()));
+    RC(set_smem(k_fused_iter<NQ, T, Acc>, lay.bytes(), s->max_smem));
     constexpr int RPT = sizeof(T) == 4 ? 2 : 1;
-    RC(set_smem(k_pcg_rows<NQ, T, Acc, RPT>, RowPcg<NQ, RPT>::template smem_bytes<T>(s->N)));
+    RC(set_smem(k_pcg_rows<NQ, T, Acc, RPT>, RowPcg<NQ, RPT>::template smem_bytes<T>(s->N),
+                s->max_smem));
     return GATO_OK;
 }
 
