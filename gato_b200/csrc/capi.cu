@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -1234,3 +1235,124 @@ int gato_stage_pcg(gato_solver_t* s, void* stream, const float* d_S, const float
 }
 
 }  // extern "C"
+
+// --- batched PCG with no device allocation -------------------------------------
+// A model-predictive controller that re-solves every millisecond cannot call
+// cudaMalloc inside its control loop: the call may synchronise the whole
+// device and its latency has no bound.  Hosts whose device memory belongs to
+// another allocator (a framework's pool, a pre-reserved real-time budget)
+// cannot let a library allocate either.  gato_pcg_static runs the PCG stage
+// of gato_stage_pcg on caller-owned buffers without a solver handle.  The
+// only device scratch that PCG kernel needs besides its operands (one
+// "already converged" flag and one stopping tolerance per problem) lives in
+// the file-scope array below instead of solver-owned buffers.
+namespace {
+
+constexpr int PCG_STATIC_MAX_BATCH = GATO_PCG_STATIC_MAX_BATCH;
+// [0, 4*MAX): int converged flags, [4*MAX, 8*MAX): float tolerances (64 KiB)
+constexpr size_t PCG_STATIC_SCRATCH_BYTES =
+    (size_t)PCG_STATIC_MAX_BATCH * (sizeof(int) + sizeof(float));
+static __device__ __align__(256) unsigned char g_pcg_scratch[PCG_STATIC_SCRATCH_BYTES];
+
+constexpr int PCG_STATIC_MAX_DEVICES = 64;
+struct PcgStaticDevice {
+    bool ready = false;
+    unsigned char* scratch = nullptr;  // device address of g_pcg_scratch
+    int max_smem = 0;
+};
+PcgStaticDevice g_pcg_static[PCG_STATIC_MAX_DEVICES];
+std::mutex g_pcg_static_mu;
+
+// flags := 0 (no problem is skipped), tolerances := pcg_tol
+__global__ void k_pcg_static_init(int* conv, float* tol, int B, float pcg_tol)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < B) {
+        conv[b] = 0;
+        tol[b] = pcg_tol;
+    }
+}
+
+// One-time set-up per device, run with that device current: look up the
+// device address of the scratch array and raise the PCG kernels' shared
+// memory limit (the same value configure_kernels sets).
+int pcg_static_setup(int dev, PcgStaticDevice** out)
+{
+    std::lock_guard<std::mutex> lock(g_pcg_static_mu);
+    PcgStaticDevice& d = g_pcg_static[dev];
+    if (!d.ready) {
+        void* p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_pcg_scratch));
+        int sm = 0;
+        CK(cudaDeviceGetAttribute(&sm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        CK(cudaFuncSetAttribute(k_pcg<6, float, float>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        CK(cudaFuncSetAttribute(k_pcg<7, float, float>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        d.scratch = static_cast<unsigned char*>(p);
+        d.max_smem = sm;
+        d.ready = true;
+    }
+    *out = &d;
+    return GATO_OK;
+}
+
+template <int NQ>
+int pcg_static_launch(const PcgStaticDevice& d, cudaStream_t st, int N, int B, float pcg_tol,
+                      int max_pcg_iters, const float* S, const float* Pinv, const float* gamma,
+                      float* lambda, int32_t* iters)
+{
+    int* conv = reinterpret_cast<int*>(d.scratch);
+    float* tol = reinterpret_cast<float*>(d.scratch + (size_t)PCG_STATIC_MAX_BATCH * sizeof(int));
+    const bool stage = pcg_smem_bytes<NQ, float>(N, true) <= (size_t)d.max_smem;
+    const size_t sm = pcg_smem_bytes<NQ, float>(N, stage);
+    if (sm > (size_t)d.max_smem)
+        return fail(GATO_ERR_UNSUPPORTED, "N=%d needs %zu bytes of shared memory", N, sm);
+    Batch<NQ, float> bt{};
+    bt.B = B;
+    bt.N = N;
+    bt.max_pcg_iters = max_pcg_iters;
+    bt.S = const_cast<float*>(S);
+    bt.P = const_cast<float*>(Pinv);
+    bt.gamma = const_cast<float*>(gamma);
+    bt.lambda = lambda;
+    bt.pcg_iters = iters;
+    bt.conv = conv;
+    bt.tol = tol;
+    k_pcg_static_init<<<cdiv(B, 256), 256, 0, st>>>(conv, tol, B, pcg_tol);
+    CKL();
+    k_pcg<NQ, float, float><<<B, PCG_THREADS, sm, st>>>(bt, stage, -1);
+    CKL();
+    return GATO_OK;
+}
+
+}  // namespace
+
+extern "C" int gato_pcg_static(void* stream, int nq, int N, int batch, float pcg_tol,
+                               int max_pcg_iters, const float* d_S, const float* d_Pinv,
+                               const float* d_gamma, float* d_lambda, int32_t* d_iters)
+{
+    if (nq != 6 && nq != 7) return fail(GATO_ERR_UNSUPPORTED, "nq=%d: built for 6 or 7", nq);
+    if (N < 2 || N > 256) return fail(GATO_ERR_ARG, "N=%d out of range [2, 256]", N);
+    if (batch < 1 || batch > PCG_STATIC_MAX_BATCH)
+        return fail(GATO_ERR_ARG, "batch=%d out of range [1, %d] of the static scratch", batch,
+                    PCG_STATIC_MAX_BATCH);
+    if (max_pcg_iters < 0) return fail(GATO_ERR_ARG, "negative max_pcg_iters");
+    if (!d_S || !d_Pinv || !d_gamma || !d_lambda || !d_iters)
+        return fail(GATO_ERR_ARG, "null device buffer");
+    if (((uintptr_t)d_S | (uintptr_t)d_Pinv) & 15)
+        return fail(GATO_ERR_ARG, "S and Pinv must be 16-byte aligned");
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= PCG_STATIC_MAX_DEVICES)
+        return fail(GATO_ERR_UNSUPPORTED, "device %d beyond the %d supported", dev,
+                    PCG_STATIC_MAX_DEVICES);
+    PcgStaticDevice* d = nullptr;
+    RC(pcg_static_setup(dev, &d));
+    cudaStream_t st = as_stream(stream);
+    if (nq == 6)
+        return pcg_static_launch<6>(*d, st, N, batch, pcg_tol, max_pcg_iters, d_S, d_Pinv,
+                                    d_gamma, d_lambda, d_iters);
+    return pcg_static_launch<7>(*d, st, N, batch, pcg_tol, max_pcg_iters, d_S, d_Pinv, d_gamma,
+                                d_lambda, d_iters);
+}

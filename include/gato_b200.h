@@ -270,6 +270,27 @@ int gato_stage_pcg(gato_solver_t* s, void* stream, const float* d_S,
                    const float* d_Pinv, const float* d_gamma, float* d_lambda,
                    int32_t* d_iters);
 
+/* No counterpart in the reference.  The PCG of gato_stage_pcg (FP32 arithmetic
+   and reductions, every problem solved) on caller-owned device buffers, with
+   no solver handle and no device allocation, for callers that may not
+   allocate: a control loop re-solving every millisecond cannot afford
+   cudaMalloc's device-wide synchronisation, and some hosts hand all device
+   memory to their own allocator.  Same buffer layout as gato_stage_pcg;
+   d_S and d_Pinv 16-byte aligned; nq 6 or 7, 2 <= N <= 256,
+   1 <= batch <= GATO_PCG_STATIC_MAX_BATCH (larger batches return
+   GATO_ERR_ARG).  The per-problem scratch (converged flags and tolerances,
+   GATO_PCG_STATIC_MAX_BATCH * 8 bytes) is one static device array in the
+   library; every call re-initialises the part it uses on `stream` before the
+   solve, so nothing has to start at zero.  Because the scratch is shared,
+   calls on one device must not overlap: two calls in flight at once (other
+   streams or host threads) race on it.  The first call on each device does
+   a one-time set-up (scratch address lookup, kernel attribute) with that
+   device current; make that first call before any stream capture begins. */
+#define GATO_PCG_STATIC_MAX_BATCH 8192
+int gato_pcg_static(void* stream, int nq, int N, int batch, float pcg_tol,
+                    int max_pcg_iters, const float* d_S, const float* d_Pinv,
+                    const float* d_gamma, float* d_lambda, int32_t* d_iters);
+
 #ifdef __cplusplus
 }
 #endif
