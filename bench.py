@@ -35,6 +35,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PLANT, N, DT = "iiwa14", 32, 0.01
+# DRAM bytes (read + write) per launch from one ncu capture of the first SQP
+# iteration of this workload (profiles/k_fused_iter_iiwa14_N32_B1024.md,
+# profiles/k_pcg_rows_iiwa14_N32_B1024.md)
+TRAFFIC_PER_LAUNCH = {"fused_iter": 239_061_504, "pcg": 237_881_088}
+KERNEL_NAMES = {"fused_iter": "k_fused_iter", "pcg": "k_pcg_rows", "line_search": "k_merit_ls",
+                "merit": "k_merit_ls (one step size)"}
 SQP_ITERS, PCG_MAX, PCG_TOL = 5, 173, 1e-5
 METRIC = "SQP solves/s (iiwa14 N=32, batch 1024, 5 SQP iters, PCG tol 1e-5)"
 WORKLOAD = ("iiwa14 N=32 dt=0.01, batch 1024 per GPU, seeded figure-8 goals, perturbed "
@@ -52,7 +58,7 @@ def solver_kwargs():
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=1024)
@@ -81,24 +87,52 @@ def make_workload(batch, seed):
     return dict(xs=pr["xs"], goal=pr["goal"], xu=xu0, lam=lam)
 
 
-def pcg_flops(pcg_iters, nx=14):
-    """Algorithmic FLOPs of the PCG iterations: per iteration two block-
-    tridiagonal matvecs (2 * N * nx * 3nx multiply-adds each) plus the dot
-    products and vector updates (about 10 flops per padded entry)."""
-    per_it = 2 * (2 * N * nx * 3 * nx) + 10 * (N + 2) * nx
-    return float(np.sum(pcg_iters)) * per_it
+# Per-knot FLOPs of the reference's own device functions for iiwa14, counted
+# by running them with an operation-counting scalar type
+# (oracle/ref_shim/flop_count.cpp, built by oracle/build_ref.py; the CPU
+# tests re-derive these numbers when that counter is built).
+REF_KNOT_FLOPS = {"kkt_dynamics": 45716, "kkt_cost": 13165, "merit_cost": 1006,
+                  "merit_defect": 12882}
 
 
-def knot_flops(nx=14, nu=7):
-    """Algorithmic FLOPs per SQP iteration per problem outside the PCG:
-    Schur complement and preconditioner ((N-1) knots: three Gauss-Jordan
-    inverses of 2n^2(n+1) flops, theta/phi/gamma products, the preconditioner
-    off-diagonal product) and step recovery."""
+def schur_flops(nx=14, nu=7):
+    """Schur complement, preconditioner and gamma of one problem
+    (schur_linsys.cuh:54-260 restated): per knot two n x n and one m x m
+    Gauss-Jordan inverses (2k^2(k+1) flops each), the theta / phi products
+    and the preconditioner's off-diagonal product."""
     gj = lambda n: 2 * n * n * (n + 1)
-    schur = (N - 1) * (2 * gj(nx) + gj(nu) + 2 * (nx ** 3) * 2 + 2 * nx * nu * nu
-                       + 2 * nx * nx * nu + 4 * nx * nx + 4 * nx ** 3)
-    dz = N * (2 * nx * nx * 2 + 2 * nx * nu * 2 + 2 * nu * nu)
-    return schur + dz
+    return (N - 1) * (2 * gj(nx) + gj(nu) + 2 * (nx ** 3) * 2 + 2 * nx * nu * nu
+                      + 2 * nx * nx * nu + 4 * nx * nx + 4 * nx ** 3)
+
+
+def dz_flops(nx=14, nu=7):
+    """Step recovery of one problem (schur_linsys.cuh:312-431)."""
+    return N * (2 * nx * nx * 2 + 2 * nx * nu * 2 + 2 * nu * nu)
+
+
+def pcg_iter_flops(nx=14):
+    """One PCG iteration of one problem: two block-tridiagonal matvecs
+    (N block rows of n x 3n multiply-adds each) plus the dot products and
+    vector updates (about 10 flops per padded entry)."""
+    return 2 * (2 * N * nx * 3 * nx) + 10 * (N + 2) * nx
+
+
+def kernel_flops(B, pcg_iters, launches):
+    """Algorithmic FLOPs of each fused-form kernel over one solve:
+    fused_iter  KKT blocks of every knot (dynamics, derivatives, cost) and
+                the Schur system, per SQP iteration
+    pcg         the PCG iterations actually run, plus step recovery
+    line_search 8 step sizes x N knots of cost + integrator defect
+    merit       the initial and final merits (one step size)"""
+    F = REF_KNOT_FLOPS
+    knot_kkt = F["kkt_dynamics"] + F["kkt_cost"]
+    knot_merit = F["merit_cost"] + F["merit_defect"]
+    return {
+        "fused_iter": launches["fused_iter"] * B * (N * knot_kkt + schur_flops()),
+        "pcg": float(np.sum(pcg_iters)) * pcg_iter_flops() + launches["pcg"] * B * dz_flops(),
+        "line_search": launches["line_search"] * B * 8 * N * knot_merit,
+        "merit": launches["merit"] * B * N * knot_merit,
+    }
 
 
 class ClockSampler:
@@ -215,6 +249,7 @@ def run_reference(args):
         v, dt = cpu_baseline(wl, sample, threads)
         times.append(dt)
     value = args.steps * sample / float(np.sum(times))
+    ref_gpu = reference_gpu_leg(args)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -228,9 +263,79 @@ def run_reference(args):
                                    f"no CPU implementation)"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "reference_gpu": ref_gpu,
     }
     print(json.dumps(line))
     return 0
+
+
+def reference_gpu_leg(args):
+    """The reference's own CUDA solver (python/bindings.cu compiled unmodified
+    for sm_100a into oracle/_ref by oracle/build_ref_gpu.py) on the same
+    workload, through its own solve(): host arrays in, host arrays out, as
+    its Python interface calls it.  Reported beside the CPU arm; absent
+    module or GPU gives an "unavailable" entry."""
+    import glob
+    import importlib.util
+    paths = glob.glob(os.path.join(ROOT, "oracle", "_ref", f"bsqpN{N}_{PLANT}*.so"))
+    if not paths:
+        return {"unavailable": "reference CUDA module not built (oracle/build_ref_gpu.py)"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no GPU"}
+        torch.cuda.init()
+    except ImportError:
+        return {"unavailable": "torch missing"}
+    name = f"bsqpN{N}_{PLANT}"
+    spec = importlib.util.spec_from_file_location(name, paths[0])
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    B = args.batch
+    cls = getattr(mod, f"BSQP_{B}_float", None)
+    if cls is None:
+        return {"unavailable": f"the reference module has no batch-{B} class"}
+    from gato_b200 import workloads as W
+
+    def make(kw):
+        return cls(DT, kw["max_sqp_iters"], kw["kkt_tol"], kw["max_pcg_iters"], kw["pcg_tol"],
+                   kw["solve_ratio"], kw["mu"], kw["q_cost"], kw["qd_cost"], kw["u_cost"],
+                   kw["N_cost"], kw["q_lim_cost"], kw["vel_lim_cost"], kw["ctrl_lim_cost"],
+                   kw["rho"])
+
+    # warm start made as for the other arms: the seeded problems solved to
+    # convergence from the default warm start (here by the reference itself),
+    # then the same seeded perturbation
+    pr = W.make_problem(PLANT, N, B, seed=2026, goals="figure8", dt=DT)
+    kw = solver_kwargs()
+    kw30 = dict(kw, max_sqp_iters=30, pcg_tol=1e-6, max_pcg_iters=400)
+    conv = make(kw30)
+    f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+    res = conv.solve(f32(pr["xu"]), DT, f32(pr["xs"]), f32(pr["goal"]))
+    del conv
+    xu0 = W.perturb(np.array(res["XU"]), 7, N, pr["rng"]).astype(np.float32)
+    xu0[:, :14] = pr["xs"]
+    xs, goal = f32(pr["xs"]), f32(pr["goal"])
+    solver = make(kw)
+    wall, own = [], []
+    for i in range(args.warmup + args.steps):
+        solver.reset_rho()
+        xin = xu0.copy()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = solver.solve(xin, DT, xs, goal)
+        t1 = time.perf_counter()
+        if i >= args.warmup:
+            wall.append(t1 - t0)
+            own.append(float(out["sqp_time_us"]) * 1e-6)
+    pcg = np.array(out["pcg_iters"])
+    return {"value": B / float(np.mean(wall)), "unit": "solves/s",
+            "own_timer_value": B / float(np.mean(own)),
+            "ms_per_step": 1e3 * float(np.mean(wall)),
+            "kind": "reference CUDA build, FP32 -use_fast_math, sm_100a",
+            "note": "solve() with host arrays (its own H2D/D2H inside); lambda carried "
+                    "between calls as the reference keeps it; rho reset before each call",
+            "pcg_iters_mean": float(pcg.mean()) if pcg.size else None}
 
 
 def make_cpu_workload(batch, sample, threads):
@@ -396,12 +501,15 @@ def run_ours(args):
 
     traj = wl["xu"].shape[1]
     solves = world * B
-    flops_pcg = pcg_flops(st["pcg_iters"])
-    iters_run = st["ls_num_iters"] + (1 if st["ls_num_iters"] < SQP_ITERS else 0)
-    flops_other = knot_flops() * B * iters_run
-    fi = kern["fused_iter"]
-    fi_ms = fi["ms"] / max(1, fi["launches"])
-    achieved = (flops_pcg + flops_other) / max(1, fi["launches"]) / (fi_ms * 1e-3) / 1e12
+    launches = {k: v["launches"] for k, v in kern.items()}
+    flops = kernel_flops(B, st["pcg_iters"], launches)
+    roof = {}
+    for k, f in flops.items():
+        if kern[k]["launches"]:
+            ms = kern[k]["ms"] / kern[k]["launches"]
+            tf = f / kern[k]["launches"] / (ms * 1e-3) / 1e12
+            roof[k] = {"ms_per_launch": ms, "tflops": tf, "frac": tf / fp32_peak}
+    top = max(roof, key=lambda k: kern[k]["ms"])
     line = {
         "metric": METRIC,
         "value": solves / (ms_fused * 1e-3),
@@ -430,10 +538,15 @@ def run_ours(args):
         "gpu_launches": int(sum(v["launches"] for v in kern.values())) * args.steps,
         "kernels_ms": {k: round(v["ms"], 4) for k, v in kern.items() if v["launches"]},
         "pcg_iters_mean": float(np.mean(st["pcg_iters"])),
-        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                     "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
-                     "kernel": "k_fused_iter", "peak_source": "measured SGEMM (TF32 off)",
+        "roofline": {"bound": "fp32", "achieved": roof[top]["tflops"], "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": roof[top]["frac"],
+                     "traffic": TRAFFIC_PER_LAUNCH.get(top),
+                     "kernel": KERNEL_NAMES[top],
+                     "peak_source": "measured FP32 SGEMM on this GPU (TF32 off)",
+                     "flops_source": "reference device functions run with a counting scalar",
                      "hbm_peak_gbs": peaks.get("hbm_gbs")},
+        "roofline_by_kernel": {KERNEL_NAMES[k]: {kk: round(vv, 4) for kk, vv in v.items()}
+                               for k, v in roof.items()},
         "clocks": clk,
     }
     if cpu is not None:

@@ -111,7 +111,10 @@ def filter_grid(text):
     return "".join(out)
 
 
-def build(plant):
+def build(plant, program="grid_ref_wrap.cpp"):
+    """Compiles ref_shim/<program> against the filtered reference headers:
+    the shared library libgrid_ref_<plant>.so for grid_ref_wrap.cpp, the
+    executable flop_count_<plant> for flop_count.cpp."""
     tmp = tempfile.mkdtemp(prefix="gato_ref_")
     try:
         gato = os.path.join(tmp, "gato")
@@ -130,15 +133,17 @@ def build(plant):
             with open(dst, "w") as f:
                 f.write(text)
         os.makedirs(OUT, exist_ok=True)
-        lib = os.path.join(OUT, f"libgrid_ref_{plant}.so")
+        shared = program == "grid_ref_wrap.cpp"
+        lib = os.path.join(OUT, f"libgrid_ref_{plant}.so" if shared else
+                           f"{os.path.splitext(program)[0]}_{plant}")
         flag = "PLANT_IIWA14" if plant == "iiwa14" else "PLANT_INDY7"
         cmd = [
-            "g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-w",
+            "g++", "-std=c++17", "-O2", "-fPIC", "-w"] + (["-shared"] if shared else []) + [
             f"-D{flag}=1", "-DKNOT_POINTS=32", "-DNDEBUG",
             "-I", os.path.join(HERE, "ref_shim", "stub"),
             "-I", gato,
             "-include", "cuda_runtime.h",
-            os.path.join(HERE, "ref_shim", "grid_ref_wrap.cpp"),
+            os.path.join(HERE, "ref_shim", program),
             "-o", lib,
         ]
         subprocess.run(cmd, check=True)
@@ -154,6 +159,7 @@ def main(argv):
         return 0
     for p in plants:
         print(build(p))
+        print(build(p, "flop_count.cpp"))
     return 0
 
 
