@@ -362,6 +362,28 @@ def make_cpu_workload(batch, sample, threads):
 
 
 # --------------------------------------------------------------------------
+def replica_seed(rank):
+    """Seed of the problems a rank solves: every GPU runs an independent
+    replica batch (problems do not interact, so the batch shards with no
+    data-path collective)."""
+    return 2026 + rank
+
+
+def max_over_ranks(x, dist=None, device=None):
+    """The slowest rank's value of a per-rank time (all ranks take part)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_solves_per_s(world, batch, ms_per_step):
+    """Whole-job throughput: every rank's batch over the slowest rank's time."""
+    return world * batch / (ms_per_step * 1e-3)
+
+
 def time_device_steps(torch, solver, bufs, wl, steps, warmup, flush, stream):
     """Per-step CUDA-event times of solver.solve_device (fused graph or plain
     driver) with warm-start state restored and L2 flushed between steps."""
@@ -404,7 +426,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=dev)
     B = args.batch
-    wl = make_workload(B, seed=2026 + rank)
+    wl = make_workload(B, seed=replica_seed(rank))
     kw = solver_kwargs()
     fused = gato_b200.BSQP(batch_size=B, N=N, dt=DT, plant_type=PLANT, form="fused",
                            precision=args.precision, **kw)
@@ -471,19 +493,11 @@ def run_ours(args):
             e2e_times.append(t1 - t0)
     e2e_times = np.array(e2e_times)
 
-    # max over ranks
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    ms_fused = max_over_ranks(float(np.mean(t_fused)))
-    ms_plain = max_over_ranks(float(np.mean(t_plain)))
-    s_e2e = max_over_ranks(float(np.mean(e2e_times)))
-    p50 = max_over_ranks(float(np.median(t_fused)))
-    p99 = max_over_ranks(float(np.percentile(t_fused, 99)))
+    ms_fused = max_over_ranks(float(np.mean(t_fused)), dist, dev)
+    ms_plain = max_over_ranks(float(np.mean(t_plain)), dist, dev)
+    s_e2e = max_over_ranks(float(np.mean(e2e_times)), dist, dev)
+    p50 = max_over_ranks(float(np.median(t_fused)), dist, dev)
+    p99 = max_over_ranks(float(np.percentile(t_fused, 99)), dist, dev)
 
     # CPU baseline (rank 0, N=1 only)
     cpu = None
@@ -512,7 +526,7 @@ def run_ours(args):
     top = max(roof, key=lambda k: kern[k]["ms"])
     line = {
         "metric": METRIC,
-        "value": solves / (ms_fused * 1e-3),
+        "value": aggregate_solves_per_s(world, B, ms_fused),
         "unit": "solves/s",
         "n_gpus": world,
         "steps": args.steps,
