@@ -169,6 +169,8 @@ struct gato_solver {
     double dt = 0.01;
     int adapt_rho = 1;
     int use_fext = 0;
+    void* wdiag = nullptr;  // [B][nx+nu] diagonal cost weights, allocated on first use
+    int use_wdiag = 0;
     int max_smem = 0;
     // device memory, scalar-typed buffers as raw pointers
     void *xu = nullptr, *xs = nullptr, *goal = nullptr, *fext = nullptr;
@@ -254,6 +256,7 @@ Batch<Tg::NQ, typename Tg::T> make_batch(gato_solver* s, void* xu, const void* x
     b.N = s->N;
     b.solve_ratio = (float)s->params.solve_ratio;
     b.max_pcg_iters = s->params.max_pcg_iters;
+    b.abs_tol = 1e-6f;
     b.adapt_rho = s->adapt_rho;
     b.cp.dt = (T)s->dt;
     b.cp.q_cost = (T)s->params.q_cost;
@@ -268,6 +271,7 @@ Batch<Tg::NQ, typename Tg::T> make_batch(gato_solver* s, void* xu, const void* x
     b.goal = (const T*)goal;
     b.fext = (const T*)s->fext;
     b.use_fext = s->use_fext;
+    b.cp.wdiag = s->use_wdiag ? (const T*)s->wdiag : nullptr;
     b.Q = (T*)s->Q;
     b.R = (T*)s->R;
     b.q = (T*)s->q;
@@ -1014,6 +1018,26 @@ int gato_set_f_ext_batch(gato_solver_t* s, const float* h_f_ext)
     return GATO_OK;
 }
 
+int gato_set_cost_diag_batch(gato_solver_t* s, const float* h_wdiag)
+{
+    RC(check_handle(s));
+    RC(bind_device(s));
+    const int use = h_wdiag != nullptr;
+    if (use) {
+        const size_t n = (size_t)3 * s->nq * s->B;
+        std::vector<double> v(h_wdiag, h_wdiag + n);
+        for (double x : v)
+            if (!std::isfinite(x)) return fail(GATO_ERR_ARG, "non-finite cost weight");
+        if (!s->wdiag) RC(s->alloc_t(&s->wdiag, n));
+        RC(s->upload(s->wdiag, v.data(), n));
+    }
+    if (use != s->use_wdiag) {
+        s->use_wdiag = use;
+        s->version++;
+    }
+    return GATO_OK;
+}
+
 int gato_set_rho_penalty_batch(gato_solver_t* s, const float* h_rho, int set_as_reset_default)
 {
     RC(check_handle(s));
@@ -1312,6 +1336,7 @@ int pcg_static_launch(const PcgStaticDevice& d, cudaStream_t st, int N, int B, f
     bt.B = B;
     bt.N = N;
     bt.max_pcg_iters = max_pcg_iters;
+    bt.abs_tol = 1e-6f;
     bt.S = const_cast<float*>(S);
     bt.P = const_cast<float*>(Pinv);
     bt.gamma = const_cast<float*>(gamma);

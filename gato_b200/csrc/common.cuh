@@ -36,12 +36,27 @@ struct DevModel {
     int barrier_style;  // 0 exact barrier Hessian, 1 outer product of gradients
 };
 
-// Cost weights and time step, as in the BSQP constructor.
+// Cost weights and time step, as in the BSQP constructor.  `wdiag`, when
+// set, holds one problem's diagonal state and control weights
+// [Qd_0..Qd_{nx-1}, Rd_0..Rd_{nu-1}]: the cost gains 1/2 Qd_i x_i^2 on every
+// state entry and 1/2 Rd_i u_i^2 on every control, replacing the uniform
+// qd_cost (velocities) and u_cost.  With Qd = [0, qd_cost], Rd = u_cost it is
+// the reference's cost (iiwa14_plant.cuh:275-424).
 template <typename T>
 struct CostParams {
     T dt;
     T q_cost, qd_cost, u_cost, N_cost, q_lim_cost, vel_lim_cost, ctrl_lim_cost;
+    const T* wdiag;
 };
+
+// the cost parameters of problem b (offsets the per-problem weights)
+template <int NQ, typename T>
+__device__ __forceinline__ CostParams<T> cost_of(const CostParams<T>& cp, int b)
+{
+    CostParams<T> c = cp;
+    if (c.wdiag) c.wdiag += (size_t)b * 3 * NQ;
+    return c;
+}
 
 // precision-generic math
 __device__ __forceinline__ void gsincos(float x, float* s, float* c) { sincosf(x, s, c); }

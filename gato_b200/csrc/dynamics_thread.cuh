@@ -244,11 +244,12 @@ __device__ __forceinline__ T merit_thread(const DevModel<NQ, T>& M, const CostPa
     T cost = T(0);
 #pragma unroll
     for (int i = 0; i < NQ; ++i) {
-        cost += T(0.5) * cp.qd_cost * qd[i] * qd[i];
+        cost += T(0.5) * (cp.wdiag ? cp.wdiag[NQ + i] : cp.qd_cost) * qd[i] * qd[i];
+        if (cp.wdiag) cost += T(0.5) * cp.wdiag[i] * q[i] * q[i];
         cost += cp.q_lim_cost * barrier(q[i], M.qlo[i], M.qhi[i]);
         cost += cp.vel_lim_cost * barrier(qd[i], M.vlo[i], M.vhi[i]);
         if (!last) {
-            cost += T(0.5) * cp.u_cost * u[i] * u[i];
+            cost += T(0.5) * (cp.wdiag ? cp.wdiag[nx + i] : cp.u_cost) * u[i] * u[i];
             cost += cp.ctrl_lim_cost * barrier(u[i], M.ulo[i], M.uhi[i]);
         }
     }

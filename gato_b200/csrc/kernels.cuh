@@ -21,6 +21,7 @@ struct Batch {
     int B, N;
     float solve_ratio;
     int max_pcg_iters;
+    float abs_tol;  // PCG absolute floor on |r.z| (1e-6 in the reference, pcg.cuh:85-89)
     int adapt_rho;
     CostParams<T> cp;
     // problem data
@@ -61,7 +62,7 @@ __global__ void k_merit(Batch<NQ, T> bt, DevModel<NQ, T> M, int nalpha, int use_
     T* s = smem + warp_id() * MeritSmem<NQ>::SIZE;
     const Dims<NQ> d{N};
     const T alpha = T(1) / (T)(1 << j);
-    const T v = merit_knot<NQ, T>(M, bt.cp, N, k, alpha, bt.mu[b], bt.xu + (size_t)b * d.traj(),
+    const T v = merit_knot<NQ, T>(M, cost_of<NQ>(bt.cp, b), N, k, alpha, bt.mu[b], bt.xu + (size_t)b * d.traj(),
                                    use_dz ? bt.dz + (size_t)b * d.traj() : nullptr,
                                    bt.xs + (size_t)b * Dims<NQ>::nx, bt.goal + (size_t)b * d.goal(),
                                    bt.use_fext ? bt.fext + 6 * b : nullptr, s);
@@ -173,7 +174,7 @@ __global__ void __launch_bounds__(256) k_merit_ls(Batch<NQ, T> bt, DevModel<NQ, 
     for (int item = threadIdx.x; item < nalpha * N; item += blockDim.x) {
         const int k = item % N, j = item / N;
         const T alpha = T(1) / (T)(1 << j);
-        terms[item] = (Acc)merit_thread<NQ, T>(M, bt.cp, N, k, alpha, mu, xu, dz,
+        terms[item] = (Acc)merit_thread<NQ, T>(M, cost_of<NQ>(bt.cp, b), N, k, alpha, mu, xu, dz,
                                                bt.xs + (size_t)b * Dims<NQ>::nx,
                                                bt.goal + (size_t)b * d.goal(), fext);
     }
@@ -250,7 +251,7 @@ __global__ void k_kkt(Batch<NQ, T> bt, DevModel<NQ, T> M)
     const Dims<NQ> d{N};
     constexpr int nx = Dims<NQ>::nx, nu = Dims<NQ>::nu;
     T* s = smem + warp_id() * KktSmem<NQ>::SIZE;
-    kkt_knot<NQ, T>(M, bt.cp, N, k, bt.xu + (size_t)b * d.traj(), bt.xs + (size_t)b * nx,
+    kkt_knot<NQ, T>(M, cost_of<NQ>(bt.cp, b), N, k, bt.xu + (size_t)b * d.traj(), bt.xs + (size_t)b * nx,
                  bt.goal + (size_t)b * d.goal(), bt.use_fext ? bt.fext + 6 * b : nullptr,
                  bt.Q + (size_t)b * N * nx * nx, bt.R + (size_t)b * N * nu * nu,
                  bt.q + (size_t)b * N * nx, bt.r + (size_t)b * N * nu,
@@ -375,7 +376,7 @@ __device__ __forceinline__ Acc block_sum(Acc v, Acc* red)
 template <int NQ, typename T, typename Acc>
 __device__ int pcg_block(int N, const T* __restrict__ S, const T* __restrict__ P,
                          const T* __restrict__ gamma, T* __restrict__ lam, T eps, int max_iters,
-                         T* sv, Acc* red)
+                         T* sv, Acc* red, float abs_floor)
 {
     constexpr int n = 2 * NQ;
     const int L = (N + 2) * n;
@@ -400,7 +401,7 @@ __device__ int pcg_block(int N, const T* __restrict__ S, const T* __restrict__ P
     Acc part = btd_mv<NQ, T, Acc>(N, P, r, z, r);
     Acc rho = block_sum<Acc>(part, red);
     for (int i = tid; i < L; i += bs) p[i] = z[i];
-    const Acc abs_tol = Acc(1e-6);
+    const Acc abs_tol = Acc(abs_floor);
     if (fabs((double)rho) < (double)abs_tol) return 0;
     const Acc rho_init = rho < 0 ? -rho : rho;
     __syncthreads();
@@ -474,7 +475,7 @@ __global__ void k_pcg(Batch<NQ, T> bt, int stage, int it_row)
         }
         iters = pcg_block<NQ, T, Acc>(bt.N, S, P, bt.gamma + (size_t)b * d.vecp(),
                                    bt.lambda + (size_t)b * d.vecp(), bt.tol[b], bt.max_pcg_iters,
-                                   sv, red);
+                                   sv, red, bt.abs_tol);
     }
     if (threadIdx.x == 0) {
         bt.pcg_iters[b] = iters;
@@ -634,7 +635,7 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
             part += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);
         }
         Acc rho = rows_block_sum<Acc>(part, red);
-        const Acc abs_tol = Acc(1e-6);
+        const Acc abs_tol = Acc(bt.abs_tol);
         const T eps = bt.tol[b];
         if (!(fabs((double)rho) < (double)abs_tol)) {
             const Acc rho_init = rho < 0 ? -rho : rho;
@@ -880,7 +881,7 @@ __global__ void k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int 
         for (int kp = warp_id(); kp < npairs; kp += nw) {
             const int k = 2 * kp + half;
             const bool valid = k < N - 1;
-            kkt_knot<NQ, T, 16>(M, bt.cp, N, valid ? k : N - 2, xu, bt.xs + (size_t)b * nx,
+            kkt_knot<NQ, T, 16>(M, cost_of<NQ>(bt.cp, b), N, valid ? k : N - 2, xu, bt.xs + (size_t)b * nx,
                                 bt.goal + (size_t)b * d.goal(), fext, Q, R, qv, rv, A, Bm, c,
                                 ws + half * KktSmem<NQ>::SIZE, valid);
         }
@@ -917,7 +918,7 @@ __global__ void k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int 
     int iters = 0;
     if (!bt.conv[b])
         iters = pcg_block<NQ, T, Acc>(N, S, P, g, bt.lambda + (size_t)b * d.vecp(), bt.tol[b],
-                                   bt.max_pcg_iters, work, red);
+                                   bt.max_pcg_iters, work, red, bt.abs_tol);
     __syncthreads();
     for (int k = warp_id(); k < N; k += nw)
         dz_knot<NQ, T>(N, k, bt.lambda + (size_t)b * d.vecp(), Qi, Ri, qv, rv, A, Bm,

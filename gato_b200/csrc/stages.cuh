@@ -116,8 +116,9 @@ __device__ void kkt_knot(const DevModel<NQ, T>& M, const CostParams<T>& cp, int 
             T g;
             if (i < NQ) {
                 g = sg[i] * w + cp.q_lim_cost * sg[NQ + i];
+                if (cp.wdiag) g += cp.wdiag[i] * sx[i];
             } else {
-                g = cp.qd_cost * sx[i] +
+                g = (cp.wdiag ? cp.wdiag[i] : cp.qd_cost) * sx[i] +
                     cp.vel_lim_cost * barrier_grad(style, sx[i], M.vlo[i - NQ], M.vhi[i - NQ]);
             }
             qk[i] = g;
@@ -131,8 +132,9 @@ __device__ void kkt_knot(const DevModel<NQ, T>& M, const CostParams<T>& cp, int 
                     } else {
                         val += cp.q_lim_cost * sg[NQ + i] * sg[NQ + jr];
                     }
+                    if (cp.wdiag && i == jr) val += cp.wdiag[i];
                 } else {
-                    val = (i == jr) ? cp.qd_cost : T(0.0);
+                    val = (i == jr) ? (cp.wdiag ? cp.wdiag[i] : cp.qd_cost) : T(0.0);
                     if (i == jr) {
                         if (style == 0) {
                             val += cp.vel_lim_cost * barrier_hess(sx[i], M.vlo[i - NQ], M.vhi[i - NQ]);
@@ -147,10 +149,11 @@ __device__ void kkt_knot(const DevModel<NQ, T>& M, const CostParams<T>& cp, int 
         }
         if (pass == 0 && l < nu) {
             const T uu = u[l];
-            rv[k * nu + l] = cp.u_cost * uu + cp.ctrl_lim_cost * barrier_grad(style, uu, M.ulo[l], M.uhi[l]);
+            const T uw = cp.wdiag ? cp.wdiag[nx + l] : cp.u_cost;
+            rv[k * nu + l] = uw * uu + cp.ctrl_lim_cost * barrier_grad(style, uu, M.ulo[l], M.uhi[l]);
             T* Rk = R + k * nu * nu + l * nu;
             for (int jr = 0; jr < nu; ++jr) {
-                T val = (jr == l) ? cp.u_cost : T(0.0);
+                T val = (jr == l) ? uw : T(0.0);
                 if (jr == l) {
                     if (style == 0) {
                         val += cp.ctrl_lim_cost * barrier_hess(uu, M.ulo[l], M.uhi[l]);
@@ -457,12 +460,13 @@ __device__ T merit_knot(const DevModel<NQ, T>& M, const CostParams<T>& cp, int N
     T term = T(0.0);
     if (l < NQ) {
         const T v = qd[l];
-        term += T(0.5) * cp.qd_cost * v * v;
+        term += T(0.5) * (cp.wdiag ? cp.wdiag[NQ + l] : cp.qd_cost) * v * v;
+        if (cp.wdiag) term += T(0.5) * cp.wdiag[l] * q[l] * q[l];
         term += cp.q_lim_cost * barrier(q[l], M.qlo[l], M.qhi[l]);
         term += cp.vel_lim_cost * barrier(v, M.vlo[l], M.vhi[l]);
         if (!last) {
             const T uu = sx[nx + l];
-            term += T(0.5) * cp.u_cost * uu * uu;
+            term += T(0.5) * (cp.wdiag ? cp.wdiag[nx + l] : cp.u_cost) * uu * uu;
             term += cp.ctrl_lim_cost * barrier(uu, M.ulo[l], M.uhi[l]);
         }
     }

@@ -267,6 +267,31 @@ class BSQP:
         a = self._batch_arr(tol_batch)
         L.check(L.load().gato_set_pcg_tol_batch(self._h, L.fptr(a)))
 
+    def set_cost_diag_batch(self, q_diag=None, r_diag=None):
+        """Per-problem diagonal weights: q_diag [B, nx] on the state, r_diag
+        [B, nu] on the control (the stage cost gains 1/2 Qd_i x_i^2 and
+        1/2 Rd_i u_i^2 in place of the scalar qd_cost and u_cost terms).
+        Both None returns to the scalar weights.  No counterpart in the
+        reference; these are the Q/R diagonals the adjoint differentiates."""
+        if q_diag is None and r_diag is None:
+            self._wdiag = None
+            L.check(L.load().gato_set_cost_diag_batch(self._h, None))
+            return
+        B = self.batch_size
+        qd = np.broadcast_to(np.asarray(q_diag, np.float32), (B, self.nx))
+        rd = np.broadcast_to(np.asarray(r_diag, np.float32), (B, self.nu))
+        self._wdiag = np.ascontiguousarray(np.concatenate([qd, rd], axis=1), dtype=np.float32)
+        L.check(L.load().gato_set_cost_diag_batch(self._h, L.fptr(self._wdiag)))
+
+    def default_cost_diag(self):
+        """(q_diag, r_diag) equal to the scalar weights: [0, qd_cost] and
+        u_cost."""
+        B, nq = self.batch_size, self.nq
+        qd = np.zeros((B, self.nx), np.float32)
+        qd[:, nq:] = self.params.qd_cost
+        rd = np.full((B, self.nu), self.params.u_cost, np.float32)
+        return qd, rd
+
     def set_rho_adaptation(self, enabled):
         L.check(L.load().gato_set_rho_adaptation(self._h, int(bool(enabled))))
 

@@ -202,6 +202,14 @@ enum {
 int gato_profile_solve(gato_solver_t* s, void* stream, float* d_xu, const float* d_xs,
                        const float* d_goal, double* ms_by_kernel, int32_t* launches_by_kernel);
 
+/* Per-problem diagonal cost weights (no counterpart in the reference, whose
+   weights are the scalars qd_cost and u_cost): h_wdiag [B][nx+nu] =
+   [Qd_0..Qd_{nx-1}, Rd_0..Rd_{nu-1}] per problem; the stage cost gains
+   1/2 Qd_i x_i^2 and 1/2 Rd_i u_i^2 in place of 1/2 qd_cost |qd|^2 and
+   1/2 u_cost |u|^2, so Qd = [0, qd_cost], Rd = u_cost is the reference's
+   cost.  NULL returns to the scalar weights.  These are the Q/R diagonals
+   that gato_adjoint differentiates. */
+int gato_set_cost_diag_batch(gato_solver_t* s, const float* h_wdiag);
 /* Batched setters (host arrays of B floats, or 6*B for f_ext; FP64 solvers
    widen them).
    Replace BSQP::set_f_ext_batch / set_rho_penalty_batch / set_drho_batch /

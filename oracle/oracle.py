@@ -97,9 +97,9 @@ def _load():
         "orc_ee_pos": (None, [vp, _dp, _dp, _dp]),
         "orc_tracking_cost": (ctypes.c_double,
                               [vp, ctypes.POINTER(GatoParams), _dp, ctypes.c_int, _dp,
-                               ctypes.c_int]),
+                               ctypes.c_int, _dp]),
         "orc_setup_kkt": (None, [vp, ctypes.c_int, ctypes.POINTER(GatoParams), ctypes.c_double,
-                                 _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
+                                 _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
         "orc_form_schur": (None, [ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp,
                                   _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
         "orc_pcg": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp,
@@ -108,7 +108,7 @@ def _load():
                                   _dp, _dp]),
         "orc_merit": (ctypes.c_double, [vp, ctypes.c_int, ctypes.POINTER(GatoParams),
                                         ctypes.c_double, ctypes.c_double, _dp, _dp,
-                                        ctypes.c_double, _dp, _dp, _dp]),
+                                        ctypes.c_double, _dp, _dp, _dp, _dp]),
         "orc_integrate": (None, [ctypes.c_int, _dp, _dp, ctypes.c_double, _dp]),
         "orc_integrator_error": (ctypes.c_double, [vp, _dp, _dp, ctypes.c_double]),
         "orc_set_snap": (None, [ctypes.c_double]),
@@ -121,6 +121,7 @@ def _load():
         "orc_solver_set_mu": (None, [vp, _dp]),
         "orc_solver_set_tol": (None, [vp, _dp]),
         "orc_solver_set_fext": (None, [vp, _dp]),
+        "orc_solver_set_cost_diag": (None, [vp, _dp]),
         "orc_solver_set_adapt": (None, [vp, ctypes.c_int]),
         "orc_solver_reset_dual": (None, [vp]),
         "orc_solver_reset_rho": (None, [vp]),
@@ -228,11 +229,11 @@ class Model:
             return p, J.reshape(self.nq, 3).T.copy()
         return p
 
-    def tracking_cost(self, params, xu, goal, has_u=True, terminal=False):
+    def tracking_cost(self, params, xu, goal, has_u=True, terminal=False, wdiag=None):
         return lib().orc_tracking_cost(self.h, ctypes.byref(params), _p(_f64(xu)), int(has_u),
-                                       _p(_f64(goal)), int(terminal))
+                                       _p(_f64(goal)), int(terminal), _p(_f64(wdiag)))
 
-    def setup_kkt(self, N, params, dt, xu, xs, goal, fext=None):
+    def setup_kkt(self, N, params, dt, xu, xs, goal, fext=None, wdiag=None):
         """KKT blocks of one problem in the reference's memory layout: square
         and rectangular blocks are column-major, so out["A"][k, c, r] is
         A_k[r, c] (and likewise Q, R, B)."""
@@ -241,15 +242,17 @@ class Model:
                    r=np.zeros((N, m)), A=np.zeros((N, n, n)), B=np.zeros((N, m, n)),
                    c=np.zeros((N, n)))
         lib().orc_setup_kkt(self.h, N, ctypes.byref(params), dt, _p(_f64(xu)), _p(_f64(xs)),
-                            _p(_f64(goal)), _p(_f64(fext)), *[_p(out[k]) for k in "QRqrABc"])
+                            _p(_f64(goal)), _p(_f64(fext)), *[_p(out[k]) for k in "QRqrABc"],
+                            _p(_f64(wdiag)))
         return out
 
     def integrator_error(self, xux, dt, fext=None):
         return lib().orc_integrator_error(self.h, _p(_f64(xux)), _p(_f64(fext)), dt)
 
-    def merit(self, N, params, dt, mu, xu, dz, alpha, xs, goal, fext=None):
+    def merit(self, N, params, dt, mu, xu, dz, alpha, xs, goal, fext=None, wdiag=None):
         return lib().orc_merit(self.h, N, ctypes.byref(params), dt, mu, _p(_f64(xu)),
-                               _p(_f64(dz)), alpha, _p(_f64(xs)), _p(_f64(goal)), _p(_f64(fext)))
+                               _p(_f64(dz)), alpha, _p(_f64(xs)), _p(_f64(goal)), _p(_f64(fext)),
+                               _p(_f64(wdiag)))
 
 
 def form_schur(nq, N, rho, kkt):
@@ -320,6 +323,11 @@ class Solver:
 
     def set_f_ext_batch(self, v):
         lib().orc_solver_set_fext(self.h, _p(_f64(np.reshape(v, -1))))
+
+    def set_cost_diag_batch(self, wdiag):
+        """Per-problem diagonal weights [B][nx+nu] (None: the scalar weights)."""
+        lib().orc_solver_set_cost_diag(
+            self.h, None if wdiag is None else _p(_f64(np.reshape(wdiag, -1))))
 
     def set_rho_adaptation(self, on):
         lib().orc_solver_set_adapt(self.h, int(bool(on)))

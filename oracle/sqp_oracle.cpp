@@ -528,6 +528,11 @@ struct Params {
     int max_pcg_iters;
     double pcg_tol, solve_ratio, mu, q_cost, qd_cost, u_cost, N_cost, q_lim_cost,
         vel_lim_cost, ctrl_lim_cost, rho;
+    /* one problem's diagonal weights [Qd (nx), Rd (nu)] or null: the stage
+       cost gains 1/2 Qd_i x_i^2 and 1/2 Rd_i u_i^2 in place of the uniform
+       qd_cost / u_cost terms (an extension; Qd = [0, qd_cost], Rd = u_cost is
+       the reference's cost) */
+    const double* wd = nullptr;
 };
 static Params to_params(const gato_params_t* p)
 {
@@ -560,14 +565,15 @@ static double tracking_cost(const Model& m, const Params& P, const double* xu, b
     double s = 0;
     for (int i = 0; i < nq; ++i) {
         double qd = xu[i + nq];
-        s += 0.5 * P.qd_cost * qd * qd;
+        s += 0.5 * (P.wd ? P.wd[nq + i] : P.qd_cost) * qd * qd;
+        if (P.wd) s += 0.5 * P.wd[i] * xu[i] * xu[i];
         s += P.q_lim_cost * barrier(xu[i], m.qlo[i], m.qhi[i]);
         s += P.vel_lim_cost * barrier(qd, m.vlo[i], m.vhi[i]);
     }
     if (has_u)
         for (int i = 0; i < nq; ++i) {
             double u = xu[2 * nq + i];
-            s += 0.5 * P.u_cost * u * u;
+            s += 0.5 * (P.wd ? P.wd[2 * nq + i] : P.u_cost) * u * u;
             s += P.ctrl_lim_cost * barrier(u, m.ulo[i], m.uhi[i]);
         }
     double p[3];
@@ -598,15 +604,17 @@ static void tracking_grad_hess(const Model& m, const Params& P, const double* xu
         bg[i] = barrier_grad(m.barrier_style, xu[i], m.qlo[i], m.qhi[i]);
     }
     for (int i = 0; i < nx; ++i) {
-        if (i < nq)
+        if (i < nq) {
             qv[i] = ge[i] * w + P.q_lim_cost * bg[i];
-        else
-            qv[i] = P.qd_cost * xu[i] +
+            if (P.wd) qv[i] += P.wd[i] * xu[i];
+        } else {
+            qv[i] = (P.wd ? P.wd[i] : P.qd_cost) * xu[i] +
                     P.vel_lim_cost * barrier_grad(m.barrier_style, xu[i], m.vlo[i - nq], m.vhi[i - nq]);
+        }
     }
     if (computeR)
         for (int i = 0; i < nu; ++i)
-            rv[i] = P.u_cost * xu[nx + i] +
+            rv[i] = (P.wd ? P.wd[nx + i] : P.u_cost) * xu[nx + i] +
                     P.ctrl_lim_cost * barrier_grad(m.barrier_style, xu[nx + i], m.ulo[i], m.uhi[i]);
     for (int i = 0; i < nx; ++i)
         for (int j = 0; j < nx; ++j) {
@@ -618,8 +626,9 @@ static void tracking_grad_hess(const Model& m, const Params& P, const double* xu
                 } else {
                     val += P.q_lim_cost * bg[i] * bg[j];
                 }
+                if (P.wd && i == j) val += P.wd[i];
             } else {
-                val = (i == j) ? P.qd_cost : 0.0;
+                val = (i == j) ? (P.wd ? P.wd[i] : P.qd_cost) : 0.0;
                 if (i == j) {
                     if (m.barrier_style == 0)
                         val += P.vel_lim_cost * barrier_hess(xu[i], m.vlo[i - nq], m.vhi[i - nq]);
@@ -634,7 +643,7 @@ static void tracking_grad_hess(const Model& m, const Params& P, const double* xu
     if (computeR)
         for (int i = 0; i < nu; ++i)
             for (int j = 0; j < nu; ++j) {
-                double val = (i == j) ? P.u_cost : 0.0;
+                double val = (i == j) ? (P.wd ? P.wd[nx + i] : P.u_cost) : 0.0;
                 if (i == j) {
                     double uu = xu[nx + i];
                     if (m.barrier_style == 0)
@@ -1031,6 +1040,7 @@ struct Solver {
     int Bn;
     bool adapt_rho = true;
     std::vector<double> lambda, rho, drho, mu, tol, fext;
+    std::vector<double> wdiag;  // [Bn][nx+nu] when set
     std::vector<double> rho_init, drho_init;
     int threads = 1;
 };
@@ -1045,8 +1055,12 @@ static void solve(Solver& S, double dt, double* xu, const double* xs, const doub
                   SolveOut& out)
 {
     const Model& m = S.model;
-    const Params& P = S.P;
     const Dims& d = S.d;
+    /* the parameters of problem b (its diagonal weights when set) */
+    std::vector<Params> Pb(S.Bn, S.P);
+    if (!S.wdiag.empty())
+        for (int b = 0; b < S.Bn; ++b) Pb[b].wd = &S.wdiag[(size_t)b * (d.nx + d.nu)];
+    const Params& P = S.P;
     const int Bn = S.Bn, nx = d.nx, nu = d.nu, N = d.N, T = d.traj(), L = d.vecp();
     std::vector<double> Q(Bn * N * nx * nx), R(Bn * N * nu * nu), q(Bn * N * nx),
         r(Bn * N * nu), A(Bn * N * nx * nx), Bm(Bn * N * nx * nu), c(Bn * N * nx),
@@ -1060,7 +1074,7 @@ static void solve(Solver& S, double dt, double* xu, const double* xs, const doub
     const int nthr = S.threads;
     auto fext_of = [&](int b) { return &S.fext[6 * b]; };
     parallel_for(nthr, Bn, [&](int b) {
-        merit_init[b] = merit(m, P, d, dt, S.mu[b], xu + b * T, &dz[b * T], 1.0, xs + b * nx,
+        merit_init[b] = merit(m, Pb[b], d, dt, S.mu[b], xu + b * T, &dz[b * T], 1.0, xs + b * nx,
                               goal + b * 6 * N, fext_of(b));
     });
     out.initial_merit = merit_init;
@@ -1073,8 +1087,8 @@ static void solve(Solver& S, double dt, double* xu, const double* xs, const doub
             double* Ab = &A[b * N * nx * nx];
             double* Bb = &Bm[b * N * nx * nu];
             double* cb = &c[b * N * nx];
-            setup_kkt(m, P, d, dt, xu + b * T, xs + b * nx, goal + b * 6 * N, fext_of(b), Qb, Rb,
-                      qb, rb, Ab, Bb, cb);
+            setup_kkt(m, Pb[b], d, dt, xu + b * T, xs + b * nx, goal + b * 6 * N, fext_of(b), Qb,
+                      Rb, qb, rb, Ab, Bb, cb);
             form_schur(d, S.rho[b], Qb, Rb, qb, rb, Ab, Bb, cb, &Sm[b * d.b3d()],
                        &Pi[b * d.b3d()], &gam[b * L]);
             pcg_it[b] = conv[b] ? 0
@@ -1100,7 +1114,7 @@ static void solve(Solver& S, double dt, double* xu, const double* xs, const doub
             int bj = 0;
             for (int j = 0; j < NUM_ALPHAS; ++j) {
                 double a = 1.0 / (double)(1 << j);
-                double v = merit(m, P, d, dt, S.mu[b], xb, &dz[b * T], a, xs + b * nx,
+                double v = merit(m, Pb[b], d, dt, S.mu[b], xb, &dz[b * T], a, xs + b * nx,
                                  goal + b * 6 * N, fext_of(b));
                 merit_a[b * NUM_ALPHAS + j] = v;
                 if (v < best) { best = v; bj = j; }
@@ -1130,7 +1144,7 @@ static void solve(Solver& S, double dt, double* xu, const double* xs, const doub
     }
     std::fill(dz.begin(), dz.end(), 0.0);
     parallel_for(nthr, Bn, [&](int b) {
-        merit_init[b] = merit(m, P, d, dt, S.mu[b], xu + b * T, &dz[b * T], 1.0, xs + b * nx,
+        merit_init[b] = merit(m, Pb[b], d, dt, S.mu[b], xu + b * T, &dz[b * T], 1.0, xs + b * nx,
                               goal + b * 6 * N, fext_of(b));
     });
     out.final_merit = merit_init;
@@ -1186,19 +1200,22 @@ void orc_ee_pos(void* h, const double* q, double* p, double* J)
 }
 
 double orc_tracking_cost(void* h, const gato_params_t* p, const double* xu, int has_u,
-                         const double* goal, int terminal)
+                         const double* goal, int terminal, const double* wdiag)
 {
     Params P = to_params(p);
+    P.wd = wdiag;
     return tracking_cost(*(Model*)h, P, xu, has_u != 0, goal, terminal != 0);
 }
 
 void orc_setup_kkt(void* h, int N, const gato_params_t* p, double dt, const double* xu,
                    const double* xs, const double* goal, const double* fext, double* Q,
-                   double* R, double* q, double* r, double* A, double* B, double* c)
+                   double* R, double* q, double* r, double* A, double* B, double* c,
+                   const double* wdiag)
 {
     Model& m = *(Model*)h;
     Dims d{m.nq, 2 * m.nq, m.nq, N};
     Params P = to_params(p);
+    P.wd = wdiag;
     setup_kkt(m, P, d, dt, xu, xs, goal, fext, Q, R, q, r, A, B, c);
 }
 
@@ -1227,11 +1244,12 @@ void orc_compute_dz(int nq, int N, const double* lambda, const double* Qinv,
 
 double orc_merit(void* h, int N, const gato_params_t* p, double dt, double mu,
                  const double* xu, const double* dz, double alpha, const double* xs,
-                 const double* goal, const double* fext)
+                 const double* goal, const double* fext, const double* wdiag)
 {
     Model& m = *(Model*)h;
     Dims d{m.nq, 2 * m.nq, m.nq, N};
     Params P = to_params(p);
+    P.wd = wdiag;
     return merit(m, P, d, dt, mu, xu, dz, alpha, xs, goal, fext);
 }
 
@@ -1300,6 +1318,14 @@ void orc_solver_set_fext(void* h, const double* v)
 {
     Solver* S = (Solver*)h;
     S->fext.assign(v, v + 6 * S->Bn);
+}
+void orc_solver_set_cost_diag(void* h, const double* v)
+{
+    Solver* S = (Solver*)h;
+    if (v)
+        S->wdiag.assign(v, v + (size_t)S->Bn * (S->d.nx + S->d.nu));
+    else
+        S->wdiag.clear();
 }
 void orc_solver_set_adapt(void* h, int on) { ((Solver*)h)->adapt_rho = on != 0; }
 void orc_solver_reset_dual(void* h)
