@@ -7,4 +7,10 @@ include/gato_b200.h.
 from .interface import BSQP  # noqa: F401
 from ._lib import GatoError, builtin_model, load  # noqa: F401
 
-__all__ = ["BSQP", "GatoError", "builtin_model", "load"]
+__all__ = ["BSQP", "GatoError", "builtin_model", "load", "solve_differentiable"]
+
+
+def solve_differentiable(*args, **kwargs):
+    """Differentiable batched solve (gato_b200.autograd.solve_differentiable)."""
+    from .autograd import solve_differentiable as f
+    return f(*args, **kwargs)

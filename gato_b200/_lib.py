@@ -112,6 +112,10 @@ SIGNATURES = {
     "gato_stage_form_schur": (ctypes.c_int, [_vp, _vp] + [_vp] * 10),
     "gato_stage_pcg": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gato_set_cost_diag_batch": (ctypes.c_int, [_vp, _vp]),
+    "gato_adjoint": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                    ctypes.c_double, ctypes.c_int, _vp]),
+    "gato_adjoint_f64": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                        ctypes.c_double, ctypes.c_int, _vp]),
     "gato_pcg_static": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_float, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
 }

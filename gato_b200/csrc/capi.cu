@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/gato_b200.h"
+#include "adjoint.cuh"
 #include "kernels.cuh"
 #include "plant_tables.h"
 
@@ -184,6 +185,10 @@ struct gato_solver {
     int *pcg_iters = nullptr, *conv = nullptr, *sqp_iters = nullptr, *done = nullptr,
         *ls_count = nullptr, *h_pcg = nullptr;
     float *h_ls_min = nullptr, *h_ls_step = nullptr;
+    // adjoint work buffers, allocated by the first gato_adjoint call
+    void *adj_lam = nullptr, *adj_mu = nullptr, *adj_v = nullptr, *adj_scale = nullptr,
+         *adj_tol = nullptr;
+    int *adj_conv = nullptr, *adj_done = nullptr, *adj_iters = nullptr;
     // host
     std::vector<double> rho_init, drho_init;
     int* pin_i = nullptr;  // pinned host ints (B)
@@ -677,6 +682,111 @@ int do_solve(gato_solver* s, cudaStream_t st, void* xu, const void* xs, const vo
         CK(cudaMemcpy(hconv.data(), s->conv, sizeof(int) * B, cudaMemcpyDeviceToHost));
     }
     return read_stats(s, hsqp.data(), hconv.data(), rows, stats);
+}
+
+// --- adjoint ---------------------------------------------------------------------
+template <typename T>
+__global__ void k_fill(T* p, int n, T v)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+int adj_alloc(gato_solver* s)
+{
+    if (s->adj_lam) return GATO_OK;
+    const size_t B = s->B, nx = 2 * s->nq, nu = s->nq, N = s->N;
+    const size_t traj = (nx + nu) * N - nu, vecp = (N + 2) * nx;
+    RC(s->alloc_t(&s->adj_mu, B * vecp));
+    RC(s->alloc_t(&s->adj_v, B * traj));
+    RC(s->alloc_t(&s->adj_scale, B));
+    RC(s->alloc_t(&s->adj_tol, B));
+    RC(s->alloc(&s->adj_conv, B));
+    RC(s->alloc(&s->adj_done, 1));
+    RC(s->alloc(&s->adj_iters, 2 * B));
+    RC(s->alloc_t(&s->adj_lam, B * vecp));  // last: it marks the set as complete
+    return GATO_OK;
+}
+
+// PCG on (S, P^-1, bt.gamma) from bt.lambda, then the step into bt.dz
+// (residuals into bt.q, bt.r): the fused form's register PCG when it fits,
+// else the plain PCG and step kernels.
+template <class Tg>
+int pcg_and_step(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt)
+{
+    constexpr int NQ = Tg::NQ;
+    using T = typename Tg::T;
+    using Acc = typename Tg::Acc;
+    constexpr int RPT = sizeof(T) == 4 ? 2 : 1;
+    if (RowPcg<NQ, RPT>::fits(s->N)) {
+        ProfScope ps_(s, st, GATO_KERNEL_PCG);
+        k_pcg_rows<NQ, T, Acc, RPT><<<s->B, RowPcg<NQ, RPT>::threads(s->N),
+                                       RowPcg<NQ, RPT>::template smem_bytes<T>(s->N), st>>>(bt,
+                                                                                            -1);
+        CKL();
+        return GATO_OK;
+    }
+    RC(launch_pcg<Tg>(s, st, bt, -1));
+    return launch_dz<Tg>(s, st, bt);
+}
+
+// Implicit gradient of a loss of the returned trajectory xu through the QP
+// of the solver at xu (the adjoint of the converged subproblem): KKT blocks
+// recomputed at xu (dynamics derivatives are not stored), Schur system, the
+// forward QP step dz (warm-started from the solver's lambda, which is left
+// unchanged), the adjoint RHS and its PCG, then the parameter gradients.
+template <class Tg>
+int adjoint_impl(gato_solver* s, cudaStream_t st, void* xu, const void* xs, const void* goal,
+                 const void* dl, void* g_xs, void* g_goal, void* g_wdiag, double tol,
+                 int max_iters, int32_t* h_iters)
+{
+    constexpr int NQ = Tg::NQ;
+    using T = typename Tg::T;
+    const int B = s->B, N = s->N;
+    const Dims<NQ> d{N};
+    constexpr int nx = Dims<NQ>::nx, nu = Dims<NQ>::nu;
+    RC(adj_alloc(s));
+    auto bt = make_batch<Tg>(s, xu, xs, goal);
+    bt.conv = s->adj_conv;
+    bt.done = s->adj_done;
+    bt.tol = (T*)s->adj_tol;
+    bt.h_pcg = nullptr;
+    bt.max_pcg_iters = max_iters;
+    bt.abs_tol = 1e-30f;  // relative stopping only; an all-zero RHS still stops at once
+    CK(cudaMemsetAsync(s->adj_conv, 0, sizeof(int) * B, st));
+    CK(cudaMemsetAsync(s->adj_done, 0, sizeof(int), st));
+    k_fill<T><<<cdiv(B, 256), 256, 0, st>>>((T*)s->adj_tol, B, (T)tol);
+    CKL();
+    RC(launch_kkt<Tg>(s, st, bt));
+    RC(launch_schur<Tg>(s, st, bt));
+    // forward QP step at xu into s->dz
+    CK(cudaMemcpyAsync(s->adj_lam, s->lambda, s->esz * (size_t)B * d.vecp(),
+                       cudaMemcpyDeviceToDevice, st));
+    auto bf = bt;
+    bf.lambda = (T*)s->adj_lam;
+    bf.pcg_iters = s->adj_iters;
+    RC(pcg_and_step<Tg>(s, st, bf));
+    // adjoint system: RHS into q, r, gamma; PCG from zero; v into adj_v
+    k_adj_rhs<NQ, T><<<B, 256, (size_t)N * (nx + nu) * sizeof(T), st>>>(bt, (const T*)dl,
+                                                                        (T*)s->adj_scale);
+    CKL();
+    CK(cudaMemsetAsync(s->adj_mu, 0, s->esz * (size_t)B * d.vecp(), st));
+    auto ba = bt;
+    ba.lambda = (T*)s->adj_mu;
+    ba.dz = (T*)s->adj_v;
+    ba.pcg_iters = s->adj_iters + B;
+    RC(pcg_and_step<Tg>(s, st, ba));
+    constexpr int GW = 8;
+    const size_t gsm = (size_t)GW * (DynSmem<NQ>::SIZE + nx + nx + nu) * sizeof(T);
+    k_adj_grad<NQ, T><<<B, GW * WARP, gsm, st>>>(bt, dmodel<Tg>(s), (const T*)s->adj_scale,
+                                                 (const T*)s->adj_v, (const T*)s->adj_mu,
+                                                 (T*)g_xs, (T*)g_goal, (T*)g_wdiag);
+    CKL();
+    if (h_iters) {
+        CK(cudaMemcpyAsync(h_iters, s->adj_iters, sizeof(int) * 2 * B, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    return GATO_OK;
 }
 
 // sim_forward: one warp per problem (simForwardBatchedKernel,
@@ -1255,6 +1365,43 @@ int gato_stage_pcg(gato_solver_t* s, void* stream, const float* d_S, const float
         bt.S = (T*)d_S; bt.P = (T*)d_Pinv; bt.gamma = (T*)d_gamma; bt.lambda = (T*)d_lambda;
         bt.pcg_iters = d_iters;
         return launch_pcg<Tg>(s, st, bt, -1);
+    });
+}
+
+int gato_adjoint(gato_solver_t* s, void* stream, const float* d_xu, const float* d_xs,
+                 const float* d_goal, const float* d_dl_dxu, float* d_g_xs, float* d_g_goal,
+                 float* d_g_wdiag, double tol, int max_iters, int32_t* h_iters)
+{
+    RC(check_handle(s));
+    RC(check_single(s));
+    if (!d_xu || !d_xs || !d_goal || !d_dl_dxu || !d_g_xs || !d_g_goal || !d_g_wdiag)
+        return fail(GATO_ERR_ARG, "null device buffer");
+    RC(bind_device(s));
+    if (tol <= 0) tol = 1e-12;  // FP32 CG stagnates before this: it runs to its floor
+    if (max_iters <= 0) max_iters = 4 * s->N * s->nq;
+    return dispatch(s, [&](auto tg) {
+        return adjoint_impl<decltype(tg)>(s, as_stream(stream), (void*)d_xu, d_xs, d_goal,
+                                          d_dl_dxu, d_g_xs, d_g_goal, d_g_wdiag, tol, max_iters,
+                                          h_iters);
+    });
+}
+
+int gato_adjoint_f64(gato_solver_t* s, void* stream, const double* d_xu, const double* d_xs,
+                     const double* d_goal, const double* d_dl_dxu, double* d_g_xs,
+                     double* d_g_goal, double* d_g_wdiag, double tol, int max_iters,
+                     int32_t* h_iters)
+{
+    RC(check_handle(s));
+    RC(check_double(s));
+    if (!d_xu || !d_xs || !d_goal || !d_dl_dxu || !d_g_xs || !d_g_goal || !d_g_wdiag)
+        return fail(GATO_ERR_ARG, "null device buffer");
+    RC(bind_device(s));
+    if (tol <= 0) tol = 1e-20;
+    if (max_iters <= 0) max_iters = 4 * s->N * s->nq;
+    return dispatch(s, [&](auto tg) {
+        return adjoint_impl<decltype(tg)>(s, as_stream(stream), (void*)d_xu, d_xs, d_goal,
+                                          d_dl_dxu, d_g_xs, d_g_goal, d_g_wdiag, tol, max_iters,
+                                          h_iters);
     });
 }
 

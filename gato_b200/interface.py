@@ -207,9 +207,9 @@ class BSQP:
         """Solves on device buffers (torch CUDA tensors or raw pointers),
         stream-ordered; returns the stats dict (or None)."""
         st, bufs = self._stats_struct() if with_stats else (None, None)
-        L.check(L.load().gato_solve(self._h, ctypes.c_void_p(int(stream)), L.vptr(d_xu),
-                                    L.vptr(d_xs), L.vptr(d_goal),
-                                    ctypes.byref(st) if st is not None else None))
+        fn = L.load().gato_solve_f64 if self.precision == "fp64" else L.load().gato_solve
+        L.check(fn(self._h, ctypes.c_void_p(int(stream)), L.vptr(d_xu), L.vptr(d_xs),
+                   L.vptr(d_goal), ctypes.byref(st) if st is not None else None))
         if st is None:
             return None
         n, B = int(st.ls_num_iters), self.batch_size
@@ -221,6 +221,28 @@ class BSQP:
             "ls_min_merit": bufs["ls_min_merit"][: n * B].reshape(n, B),
             "ls_step_size": bufs["ls_step_size"][: n * B].reshape(n, B),
         }
+
+    def adjoint_device(self, d_xu, d_xs, d_goal, d_dl, stream=0, tol=0.0, max_iters=0,
+                       with_iters=False):
+        """Gradients of a loss of the returned trajectory d_xu (torch CUDA
+        tensors of the solver's dtype) through the QP at d_xu:
+        (g_xs [B, nx], g_goal [B, 6N], g_wdiag [B, nx+nu]) from dl/dXU
+        [B, traj] (gato_adjoint).  with_iters also returns the PCG iteration
+        counts [2, B] (forward QP step, adjoint)."""
+        import torch
+        B, dev = self.batch_size, d_xu.device
+        dt = torch.float64 if self.precision == "fp64" else torch.float32
+        g_xs = torch.empty((B, self.nx), dtype=dt, device=dev)
+        g_goal = torch.empty((B, 6 * self.N), dtype=dt, device=dev)
+        g_w = torch.empty((B, self.nx + self.nu), dtype=dt, device=dev)
+        its = np.zeros((2, B), np.int32) if with_iters else None
+        fn = L.load().gato_adjoint_f64 if self.precision == "fp64" else L.load().gato_adjoint
+        L.check(fn(self._h, ctypes.c_void_p(int(stream)), L.vptr(d_xu), L.vptr(d_xs),
+                   L.vptr(d_goal), L.vptr(d_dl), L.vptr(g_xs), L.vptr(g_goal), L.vptr(g_w),
+                   float(tol), int(max_iters), L.vptr(its)))
+        if with_iters:
+            return g_xs, g_goal, g_w, its
+        return g_xs, g_goal, g_w
 
     # -- reference helpers -----------------------------------------------
     def ee_pos(self, q):

@@ -278,6 +278,30 @@ int gato_stage_pcg(gato_solver_t* s, void* stream, const float* d_S,
                    const float* d_Pinv, const float* d_gamma, float* d_lambda,
                    int32_t* d_iters);
 
+/* Adjoint of the converged subproblem (no counterpart in the reference).
+   For a loss l of the trajectory d_xu returned by gato_solve (same x_s and
+   goals), gives dl/dx_s [B][nx], dl/dgoal [B][6N] (rpy entries 0) and
+   dl/d(Qd, Rd) [B][nx+nu] (the diagonal weights of
+   gato_set_cost_diag_batch; with scalar weights, Qd = [0, qd_cost],
+   Rd = u_cost) from d_dl_dxu [B][(nx+nu)N-nu].  The trajectory is treated
+   as xu + dz(theta), dz the solution of the QP formed at xu (exact at a
+   converged solve): the KKT blocks are recomputed at xu, the transposed KKT
+   system (the QP's own, it is symmetric) is solved through the same Schur
+   complement and PCG, and the solver's lambda and rho are left unchanged.
+   tol <= 0 / max_iters <= 0 select the defaults (relative PCG tolerance
+   1e-12 in FP32 / 1e-20 in FP64, 4*N*nq iterations).  h_iters (optional,
+   host [2][B]) receives the PCG iterations of the forward QP step and of the
+   adjoint.  The first call allocates the adjoint's work buffers. */
+int gato_adjoint(gato_solver_t* s, void* stream, const float* d_xu,
+                 const float* d_xs, const float* d_goal, const float* d_dl_dxu,
+                 float* d_g_xs, float* d_g_goal, float* d_g_wdiag, double tol,
+                 int max_iters, int32_t* h_iters);
+int gato_adjoint_f64(gato_solver_t* s, void* stream, const double* d_xu,
+                     const double* d_xs, const double* d_goal,
+                     const double* d_dl_dxu, double* d_g_xs, double* d_g_goal,
+                     double* d_g_wdiag, double tol, int max_iters,
+                     int32_t* h_iters);
+
 /* No counterpart in the reference.  The PCG of gato_stage_pcg (FP32 arithmetic
    and reductions, every problem solved) on caller-owned device buffers, with
    no solver handle and no device allocation, for callers that may not

@@ -1,0 +1,142 @@
+"""gato_adjoint against the dense FP64 reference gradient (oracle/adjoint_ref.py,
+itself pinned to central finite differences on the CPU), the per-problem
+diagonal weights against the oracle solver, and the torch.autograd.Function
+around the adjoint."""
+import numpy as np
+import pytest
+
+from helpers import nerr, problem
+
+pytestmark = pytest.mark.gpu
+
+PARAMS = dict(max_sqp_iters=5, pcg_tol=1e-5, max_pcg_iters=173, q_cost=1.5, qd_cost=1e-2,
+              u_cost=1e-3, N_cost=10.0, q_lim_cost=1e-3, rho=1e-3, mu=10.0)
+
+
+def _setup(plant, N, B, precision, seed, with_wdiag):
+    import torch
+    import gato_b200
+    torch.cuda.set_device(0)
+    pr = problem(plant, N, B, seed=seed)
+    s = gato_b200.BSQP(batch_size=B, N=N, dt=0.01, plant_type=plant, precision=precision,
+                       **PARAMS)
+    rng = np.random.default_rng(seed)
+    w = None
+    if with_wdiag:
+        w = np.exp(rng.uniform(-2, 2, (B, 3 * s.nq)))
+        s.set_cost_diag_batch(w[:, :s.nx], w[:, s.nx:])
+        w = s._wdiag.astype(np.float64)  # the weights as the solver holds them
+    dt = torch.float64 if precision == "fp64" else torch.float32
+    T = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=dt, device="cuda")
+    d_xu, d_xs, d_goal = T(pr["xu"]), T(pr["xs"]), T(pr["goal"])
+    s.solve_device(d_xu, d_xs, d_goal, with_stats=False)
+    dl = rng.normal(0, 1, (B, s.traj_size))
+    return s, pr, w, d_xu, d_xs, d_goal, T(dl), dl
+
+
+def _reference(oracle_mod, s, plant, N, b, pr, w, xu, dl):
+    from oracle import adjoint_ref as AR
+    O = oracle_mod
+    m = O.Model(plant)
+    P = O.make_params(dt=0.01, **PARAMS)
+    rho = float(s.get_rho()[b])
+    return AR.adjoint_grad(m, N, P, 0.01, xu[b].astype(np.float64),
+                           pr["xs"][b].astype(np.float64), pr["goal"][b].astype(np.float64),
+                           None if w is None else w[b], rho, dl[b])
+
+
+def _rel(a, b):
+    return float(np.abs(np.asarray(a) - b).max() / max(1e-12, np.abs(b).max()))
+
+
+def test_fp64_diagonal_weights_match_oracle_solver(oracle_mod):
+    """FP64 solve with per-problem Qd, Rd equals the oracle solver with the
+    same weights (iteration counts and trajectory)."""
+    import torch
+    import gato_b200
+    O = oracle_mod
+    plant, N, B = "iiwa14", 16, 3
+    pr = problem(plant, N, B, seed=12)
+    rng = np.random.default_rng(12)
+    s = gato_b200.BSQP(batch_size=B, N=N, dt=0.01, plant_type=plant, precision="fp64",
+                       **PARAMS)
+    w = np.exp(rng.uniform(-2, 2, (B, 21)))
+    s.set_cost_diag_batch(w[:, :14], w[:, 14:])
+    w = s._wdiag.astype(np.float64)
+    g = s.solve_raw(pr["xu"].astype(np.float64), 0.01, pr["xs"].astype(np.float64),
+                    pr["goal"].astype(np.float64))
+    S = O.Solver(plant, N, B, O.make_params(dt=0.01, **PARAMS))
+    S.set_cost_diag_batch(w)
+    xo, o = S.solve(pr["xu"].astype(np.float64), 0.01, pr["xs"], pr["goal"])
+    np.testing.assert_array_equal(g["pcg_iters"], o["pcg_iters"])
+    assert nerr(g["XU"], xo) < 1e-8
+    s.close()
+
+
+@pytest.mark.parametrize("plant,N,with_wdiag", [("iiwa14", 16, True), ("indy7", 8, False)])
+def test_fp64_adjoint_matches_dense_reference(oracle_mod, plant, N, with_wdiag):
+    B = 3
+    s, pr, w, d_xu, d_xs, d_goal, d_dl, dl = _setup(plant, N, B, "fp64", 31, with_wdiag)
+    # CG on the Schur system (condition ~1e8 here) loses orthogonality in
+    # FP64 too, so the exact-parity check allows it more than N*nx iterations
+    g_xs, g_goal, g_w, its = s.adjoint_device(d_xu, d_xs, d_goal, d_dl, max_iters=4000,
+                                              with_iters=True)
+    xu = d_xu.cpu().numpy()
+    for b in range(B):
+        r = _reference(oracle_mod, s, plant, N, b, pr, w, xu, dl)
+        errs = [_rel(g_xs[b].cpu(), r["g_xs"]), _rel(g_goal[b].cpu(), r["g_goal"]),
+                _rel(g_w[b].cpu(), r["g_wdiag"])]
+        # the adjoint's v_0 (fixed by x_0 = x_s) is a cancellation that PCG
+        # leaves at ~1e-9 absolute: 1e-5 relative bounds every component
+        assert max(errs) < 1e-5, (errs, its.tolist())
+    assert (its[1] > 0).all() and (its < 4000).all(), its.tolist()
+    s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_fp32_adjoint_close_to_dense_reference(oracle_mod, precision):
+    plant, N, B = "iiwa14", 32, 4
+    s, pr, w, d_xu, d_xs, d_goal, d_dl, dl = _setup(plant, N, B, precision, 41, True)
+    g_xs, g_goal, g_w = s.adjoint_device(d_xu, d_xs, d_goal, d_dl)
+    xu = d_xu.cpu().numpy()
+    errs = []
+    for b in range(B):
+        r = _reference(oracle_mod, s, plant, N, b, pr, w, xu, dl)
+        errs += [_rel(g_xs[b].cpu(), r["g_xs"]), _rel(g_goal[b].cpu(), r["g_goal"]),
+                 _rel(g_w[b].cpu(), r["g_wdiag"])]
+    # FP32 KKT blocks and Schur matrices carry ~1e-7 relative rounding that
+    # the KKT system (condition ~1e5 at these weights) amplifies: measured
+    # errors 1e-4 (x_s, weights) to 6e-3 (goals)
+    assert max(errs) < 2e-2 and float(np.median(errs)) < 5e-3, errs
+    s.close()
+
+
+def test_autograd_function_gradients():
+    """loss(XU).backward() reaches x0, goals and the weights, and equals the
+    direct adjoint call on the same trajectory."""
+    import torch
+    import gato_b200
+    torch.cuda.set_device(0)
+    plant, N, B = "iiwa14", 16, 2
+    pr = problem(plant, N, B, seed=5)
+    s = gato_b200.BSQP(batch_size=B, N=N, dt=0.01, plant_type=plant, precision="fp64",
+                       **PARAMS)
+    dev = torch.device("cuda")
+    x0 = torch.tensor(pr["xs"], dtype=torch.float64, device=dev, requires_grad=True)
+    goals = torch.tensor(pr["goal"], dtype=torch.float64, device=dev, requires_grad=True)
+    logq = torch.zeros((B, s.nx), dtype=torch.float64, device=dev, requires_grad=True)
+    logr = torch.full((B, s.nu), -3.0, dtype=torch.float64, device=dev, requires_grad=True)
+    xu_init = torch.tensor(pr["xu"], dtype=torch.float64, device=dev)
+    XU = gato_b200.solve_differentiable(s, x0, goals, logq.exp(), logr.exp(), xu_init)
+    target = XU.detach() + 0.1
+    loss = ((XU - target) ** 2).sum()
+    loss.backward()
+    for t in (x0, goals, logq, logr):
+        assert t.grad is not None and torch.isfinite(t.grad).all()
+    assert float(goals.grad.abs().sum()) > 0 and float(logq.grad.abs().sum()) > 0
+    g_xs, g_goal, g_w = s.adjoint_device(XU.detach().contiguous(), x0.detach(),
+                                         goals.detach(), (2 * (XU - target)).detach())
+    assert torch.allclose(x0.grad, g_xs, rtol=1e-9, atol=1e-12)
+    assert torch.allclose(goals.grad, g_goal, rtol=1e-9, atol=1e-12)
+    assert torch.allclose(logq.grad, g_w[:, :s.nx] * logq.exp(), rtol=1e-9, atol=1e-12)
+    s.close()
