@@ -493,6 +493,31 @@ def run_ours(args):
             e2e_times.append(t1 - t0)
     e2e_times = np.array(e2e_times)
 
+    # adjoint (gato_adjoint) of the fused solve's returned trajectory, timed
+    # like the forward step: CUDA events on the stream, L2 flushed between
+    # calls; the loss gradient is a seeded dense vector
+    d_xu.copy_(d_xu0)
+    fused.set_lambda(wl["lam"])
+    fused.reset_rho()
+    fused.solve_device(d_xu, d_xs, d_goal, stream=stream.cuda_stream, with_stats=False)
+    d_dl = torch.tensor(np.random.default_rng(7).normal(0, 1, tuple(d_xu.shape)),
+                        dtype=torch.float32, device=dev)
+    adj_ms, adj_its = [], None
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup + max(3, args.steps // 5)):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out = fused.adjoint_device(d_xu, d_xs, d_goal, d_dl, stream=stream.cuda_stream,
+                                       with_iters=(i == 0))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if i == 0:
+                adj_its = out[3]
+            if i >= args.warmup:
+                adj_ms.append(e0.elapsed_time(e1))
+    ms_adj = max_over_ranks(float(np.mean(adj_ms)), dist, dev)
+
     ms_fused = max_over_ranks(float(np.mean(t_fused)), dist, dev)
     ms_plain = max_over_ranks(float(np.mean(t_plain)), dist, dev)
     s_e2e = max_over_ranks(float(np.mean(e2e_times)), dist, dev)
@@ -546,6 +571,11 @@ def run_ours(args):
         "plain_form": {"value": solves / (ms_plain * 1e-3), "unit": "solves/s",
                        "ms_per_step": ms_plain},
         "fused_vs_plain": ms_plain / ms_fused,
+        "adjoint": {"ms_per_call": ms_adj, "vs_forward_solve": ms_adj / ms_fused,
+                    "pcg_iters_mean": {"forward_qp_step": float(adj_its[0].mean()),
+                                       "adjoint": float(adj_its[1].mean())},
+                    "what": "gradients for x0, goals, Q/R diagonals of a dense loss "
+                            "gradient (FP32, relative PCG tol 1e-12)"},
         "e2e": {"value": solves / s_e2e, "unit": "solves/s",
                 "h2d_bytes_per_step": int(4 * B * (traj + 14 + 6 * N)),
                 "d2h_bytes_per_step": int(4 * B * traj)},
