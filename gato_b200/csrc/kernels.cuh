@@ -572,6 +572,27 @@ __device__ __forceinline__ Acc rows_block_sum(Acc v, Acc* red)
     return s;
 }
 
+// two block sums at once (one barrier); red holds 2 * WARP slots
+template <typename Acc>
+__device__ __forceinline__ void rows_block_sum2(Acc& a, Acc& b, Acc* red)
+{
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (lane_id() == 0) {
+        red[warp_id()] = a;
+        red[WARP + warp_id()] = b;
+    }
+    __syncthreads();
+    Acc sa = 0, sb = 0;
+    const int nw = blockDim.x / WARP;
+    for (int w = 0; w < nw; ++w) {
+        sa += red[w];
+        sb += red[WARP + w];
+    }
+    a = sa;
+    b = sb;
+}
+
 template <int NQ, typename T, typename Acc, int RPT>
 __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
     k_pcg_rows(Batch<NQ, T> bt, int it_row)
@@ -629,51 +650,123 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
         }
         __syncthreads();
         rows_window_dot<NQ, RPT, T>(prow, rv + w0, z);
-#pragma unroll
-        for (int j = 0; j < RPT; ++j) {
-            p[j] = z[j];
-            part += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);
-        }
-        Acc rho = rows_block_sum<Acc>(part, red);
         const Acc abs_tol = Acc(bt.abs_tol);
         const T eps = bt.tol[b];
-        if (!(fabs((double)rho) < (double)abs_tol)) {
-            const Acc rho_init = rho < 0 ? -rho : rho;
-            for (int it = 0; it < bt.max_pcg_iters; ++it) {
-                ++iters;
-                if (act) {
-#pragma unroll
-                    for (int j = 0; j < RPT; ++j) pv[(k + 1) * VS + i0 + j * TPB] = p[j];
-                }
-                __syncthreads();
-                rows_window_dot<NQ, RPT, T>(srow, pv + w0, ap);
-                part = 0;
-#pragma unroll
-                for (int j = 0; j < RPT; ++j) part += act ? (Acc)p[j] * (Acc)ap[j] : Acc(0);
-                const Acc pap = rows_block_sum<Acc>(part, red);
-                const T alpha = (T)(rho / pap);
-#pragma unroll
-                for (int j = 0; j < RPT; ++j) {
-                    x[j] += alpha * p[j];
-                    r[j] -= alpha * ap[j];
-                    if (act) rv[(k + 1) * VS + i0 + j * TPB] = r[j];
-                }
-                __syncthreads();
-                rows_window_dot<NQ, RPT, T>(prow, rv + w0, z);
-                part = 0;
-#pragma unroll
-                for (int j = 0; j < RPT; ++j) part += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);
-                const Acc rho_new = rows_block_sum<Acc>(part, red + WARP);
-                const Acc arn = rho_new < 0 ? -rho_new : rho_new;
-                if (arn < abs_tol + (Acc)eps * rho_init) break;
-                const T beta = (T)(rho_new / rho);
-                rho = rho_new;
-#pragma unroll
-                for (int j = 0; j < RPT; ++j) p[j] = z[j] + beta * p[j];
-            }
+        if constexpr (sizeof(T) == 4) {
+            // Single-reduction form (Chronopoulos-Gear): w = S z is carried
+            // with z, s = S p by recurrence, and r.z, z.w share one block
+            // reduction, so an iteration has three barriers instead of four.
+            // Same iterates as the reference's recurrence in exact
+            // arithmetic; same stopping rule and iteration count.
+            T w[RPT], sv[RPT];
             if (act) {
 #pragma unroll
-                for (int j = 0; j < RPT; ++j) lam[(k + 1) * n + i0 + j * TPB] = x[j];
+                for (int j = 0; j < RPT; ++j) pv[(k + 1) * VS + i0 + j * TPB] = z[j];
+            }
+            __syncthreads();
+            rows_window_dot<NQ, RPT, T>(srow, pv + w0, w);
+            Acc rho = 0, delta = 0;
+#pragma unroll
+            for (int j = 0; j < RPT; ++j) {
+                rho += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);
+                delta += act ? (Acc)z[j] * (Acc)w[j] : Acc(0);
+            }
+            rows_block_sum2<Acc>(rho, delta, red);
+            if (!(fabs((double)rho) < (double)abs_tol)) {
+                const Acc rho_init = rho < 0 ? -rho : rho;
+                Acc alpha = rho / delta;
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) {
+                    p[j] = z[j];
+                    sv[j] = w[j];
+                }
+                for (int it = 0; it < bt.max_pcg_iters; ++it) {
+                    ++iters;
+                    const T a = (T)alpha;
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) {
+                        x[j] += a * p[j];
+                        r[j] -= a * sv[j];
+                        if (act) rv[(k + 1) * VS + i0 + j * TPB] = r[j];
+                    }
+                    __syncthreads();
+                    rows_window_dot<NQ, RPT, T>(prow, rv + w0, z);
+                    if (act) {
+#pragma unroll
+                        for (int j = 0; j < RPT; ++j) pv[(k + 1) * VS + i0 + j * TPB] = z[j];
+                    }
+                    __syncthreads();
+                    rows_window_dot<NQ, RPT, T>(srow, pv + w0, w);
+                    Acc rho_new = 0;
+                    delta = 0;
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) {
+                        rho_new += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);
+                        delta += act ? (Acc)z[j] * (Acc)w[j] : Acc(0);
+                    }
+                    rows_block_sum2<Acc>(rho_new, delta, red);
+                    const Acc arn = rho_new < 0 ? -rho_new : rho_new;
+                    if (arn < abs_tol + (Acc)eps * rho_init) break;
+                    const Acc beta = rho_new / rho;
+                    alpha = rho_new / (delta - beta * rho_new / alpha);
+                    rho = rho_new;
+                    const T bb = (T)beta;
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) {
+                        p[j] = z[j] + bb * p[j];
+                        sv[j] = w[j] + bb * sv[j];
+                    }
+                }
+                if (act) {
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) lam[(k + 1) * n + i0 + j * TPB] = x[j];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < RPT; ++j) {
+                p[j] = z[j];
+                part += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);
+            }
+            Acc rho = rows_block_sum<Acc>(part, red);
+            if (!(fabs((double)rho) < (double)abs_tol)) {
+                const Acc rho_init = rho < 0 ? -rho : rho;
+                for (int it = 0; it < bt.max_pcg_iters; ++it) {
+                    ++iters;
+                    if (act) {
+#pragma unroll
+                        for (int j = 0; j < RPT; ++j) pv[(k + 1) * VS + i0 + j * TPB] = p[j];
+                    }
+                    __syncthreads();
+                    rows_window_dot<NQ, RPT, T>(srow, pv + w0, ap);
+                    part = 0;
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) part += act ? (Acc)p[j] * (Acc)ap[j] : Acc(0);
+                    const Acc pap = rows_block_sum<Acc>(part, red);
+                    const T alpha = (T)(rho / pap);
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) {
+                        x[j] += alpha * p[j];
+                        r[j] -= alpha * ap[j];
+                        if (act) rv[(k + 1) * VS + i0 + j * TPB] = r[j];
+                    }
+                    __syncthreads();
+                    rows_window_dot<NQ, RPT, T>(prow, rv + w0, z);
+                    part = 0;
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) part += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);
+                    const Acc rho_new = rows_block_sum<Acc>(part, red + WARP);
+                    const Acc arn = rho_new < 0 ? -rho_new : rho_new;
+                    if (arn < abs_tol + (Acc)eps * rho_init) break;
+                    const T beta = (T)(rho_new / rho);
+                    rho = rho_new;
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) p[j] = z[j] + beta * p[j];
+                }
+                if (act) {
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) lam[(k + 1) * n + i0 + j * TPB] = x[j];
+                }
             }
         }
     }
@@ -839,7 +932,7 @@ struct FusedLayout {
 // after the Schur complement (S, P^-1 and gamma left in global memory) and
 // k_pcg_rows takes over.
 template <int NQ, typename T, typename Acc>
-__global__ void k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int it_row,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int it_row,
                              int with_pcg)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
