@@ -16,6 +16,7 @@
 #include "../../include/gato_b200.h"
 #include "adjoint.cuh"
 #include "kernels.cuh"
+#include "pcg_cluster.cuh"
 #include "plant_tables.h"
 
 using namespace gato;
@@ -447,6 +448,34 @@ int launch_ls(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::
     return GATO_OK;
 }
 
+// cluster PCG + step for horizons beyond one CTA's registers (N > ~36)
+template <class Tg>
+int launch_pcg_cluster(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt,
+                       int row)
+{
+    constexpr int NQ = Tg::NQ;
+    using T = typename Tg::T;
+    using Acc = typename Tg::Acc;
+    constexpr int RPT = sizeof(T) == 4 ? 2 : 1;
+    using CP = ClusterPcg<NQ, RPT>;
+    ProfScope ps_(s, st, GATO_KERNEL_PCG);
+    const int C = CP::ctas(s->N);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(s->B * C);
+    cfg.blockDim = dim3(CP::threads(s->N));
+    cfg.dynamicSmemBytes = CP::template smem_bytes<T>(s->N);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, k_pcg_cluster<NQ, T, Acc, RPT>, bt, row));
+    return GATO_OK;
+}
+
 template <class Tg>
 int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt,
                       int row)
@@ -472,6 +501,16 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
                                                                                             row);
         CKL();
         return GATO_OK;
+    }
+    if (ClusterPcg<NQ, RPT>::fits(s->N)) {
+        {
+            ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
+            FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, false};
+            k_fused_iter<NQ, T, Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(bt, dmodel<Tg>(s),
+                                                                              0, row, 0);
+            CKL();
+        }
+        return launch_pcg_cluster<Tg>(s, st, bt, row);
     }
     ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
     const bool stage = fused_stage_fits<Tg>(s);
@@ -726,6 +765,7 @@ int pcg_and_step(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename T
         CKL();
         return GATO_OK;
     }
+    if (ClusterPcg<NQ, RPT>::fits(s->N)) return launch_pcg_cluster<Tg>(s, st, bt, -1);
     RC(launch_pcg<Tg>(s, st, bt, -1));
     return launch_dz<Tg>(s, st, bt);
 }

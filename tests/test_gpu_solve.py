@@ -42,8 +42,10 @@ def run_pair(O, plant, N, B, params, form, precision, seed, perturbed=True, goal
 
 
 @pytest.mark.parametrize("plant,N,form", [("iiwa14", 8, "fused"), ("iiwa14", 32, "fused"),
-                                          ("iiwa14", 32, "plain"), ("indy7", 32, "fused")])
+                                          ("iiwa14", 32, "plain"), ("indy7", 32, "fused"),
+                                          ("iiwa14", 64, "fused"), ("indy7", 128, "fused")])
 def test_fp64_solve_reproduces_oracle(oracle_mod, plant, N, form):
+    """N = 64 and 128 run the cluster PCG (block rows split across CTAs)."""
     r = run_pair(oracle_mod, plant, N, 4, PARAMS_CFG2, form, "fp64", seed=31)
     g, o = r["g"], r["o"]
     assert g["ls_num_iters"] == o["ls_num_iters"]
@@ -151,14 +153,15 @@ def test_fp32_stepwise_parity_n32(oracle_mod):
     assert errs and max(errs) < 5e-3 and float(np.median(errs)) < 1e-3, errs
 
 
-def test_plain_and_fused_forms_agree():
+@pytest.mark.parametrize("N", [32, 64])
+def test_plain_and_fused_forms_agree(N):
     """The fused form evaluates the same stages with differently organised
     kernels (register-resident PCG, sample-per-thread merit), so it rounds
     differently in FP32; in FP64 both reproduce the oracle (tests above).
     One SQP iteration from identical inputs, FP32 tolerance: PCG counts equal
     for at least 75% of the problems, and where the line-search step agrees,
     XU within the PCG-limited bound 5e-3 (normalised)."""
-    plant, N, B = "iiwa14", 32, 16
+    plant, B = "iiwa14", 16
     pr = problem(plant, N, B, seed=23)
     params = dict(PARAMS_CFG2, max_sqp_iters=1)
     outs = []
