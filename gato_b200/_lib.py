@@ -61,6 +61,10 @@ class GatoParams(ctypes.Structure):
     ]
 
 
+class GatoClass(ctypes.Structure):
+    _fields_ = [("plant", ctypes.c_int), ("N", ctypes.c_int), ("count", ctypes.c_int)]
+
+
 class GatoStats(ctypes.Structure):
     _fields_ = [
         ("sqp_time_us", ctypes.c_double),
@@ -112,6 +116,18 @@ SIGNATURES = {
     "gato_stage_form_schur": (ctypes.c_int, [_vp, _vp] + [_vp] * 10),
     "gato_stage_pcg": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gato_set_cost_diag_batch": (ctypes.c_int, [_vp, _vp]),
+    "gato_mixed_create": (ctypes.c_int, [ctypes.POINTER(GatoClass), ctypes.c_int,
+                                         ctypes.POINTER(GatoParams), ctypes.c_int,
+                                         ctypes.POINTER(_vp)]),
+    "gato_mixed_destroy": (ctypes.c_int, [_vp]),
+    "gato_mixed_class": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "gato_mixed_solve": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                                        ctypes.POINTER(_vp)]),
+    "gato_mixed_stats": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(GatoStats)]),
+    "gato_mixed_elapsed_ms": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    "gato_mixed_config": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "gato_mixed_tune": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                                       ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_float)]),
     "gato_adjoint": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                     ctypes.c_double, ctypes.c_int, _vp]),
     "gato_adjoint_f64": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,

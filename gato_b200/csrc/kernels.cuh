@@ -154,16 +154,14 @@ __global__ void k_line_search(Batch<NQ, T> bt, int it, int skip_if_done)
 //   mode 1: line search over NUM_ALPHAS steps -> rho, step, XU update
 //   mode 2: merit of XU                       -> merit_final
 template <int NQ, typename T, typename Acc>
-__global__ void __launch_bounds__(256) k_merit_ls(Batch<NQ, T> bt, DevModel<NQ, T> M, int mode,
-                                                  int it)
+__device__ __forceinline__ void merit_ls_body(const Batch<NQ, T>& bt, const DevModel<NQ, T>& M,
+                                              int b, int mode, int it, unsigned char* smem_raw)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     Acc* terms = reinterpret_cast<Acc*>(smem_raw);
     __shared__ Acc s_m[NUM_ALPHAS];
     __shared__ T s_step;
     __shared__ int s_ok;
     if (mode == 1 && *bt.done) return;
-    const int b = blockIdx.x;
     const int N = bt.N;
     const int nalpha = (mode == 1) ? NUM_ALPHAS : 1;
     const Dims<NQ> d{N};
@@ -235,6 +233,14 @@ __global__ void __launch_bounds__(256) k_merit_ls(Batch<NQ, T> bt, DevModel<NQ, 
         const T st = s_step;
         for (int i = t; i < d.traj(); i += blockDim.x) x[i] += st * dz[i];
     }
+}
+
+template <int NQ, typename T, typename Acc>
+__global__ void __launch_bounds__(256) k_merit_ls(Batch<NQ, T> bt, DevModel<NQ, T> M, int mode,
+                                                  int it)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    merit_ls_body<NQ, T, Acc>(bt, M, blockIdx.x, mode, it, smem_raw);
 }
 
 // ------------------------------------------------------------------ KKT
@@ -594,14 +600,12 @@ __device__ __forceinline__ void rows_block_sum2(Acc& a, Acc& b, Acc* red)
 }
 
 template <int NQ, typename T, typename Acc, int RPT>
-__global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
-    k_pcg_rows(Batch<NQ, T> bt, int it_row)
+__device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int it_row,
+                                              unsigned char* smem_raw)
 {
     using RP = RowPcg<NQ, RPT>;
     constexpr int n = RP::n, m = RP::m, RD = RP::RD, VS = RP::VS, TPB = RP::TPB;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     if (*bt.done) return;
-    const int b = blockIdx.x;
     const int N = bt.N;
     const Dims<NQ> d{N};
     const int tid = threadIdx.x;
@@ -844,6 +848,14 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
     }
 }
 
+template <int NQ, typename T, typename Acc, int RPT>
+__global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
+    k_pcg_rows(Batch<NQ, T> bt, int it_row)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    pcg_rows_body<NQ, T, Acc, RPT>(bt, blockIdx.x, it_row, smem_raw);
+}
+
 // ------------------------------------------------------------------ dz
 template <int NQ, typename T>
 __global__ void k_dz(Batch<NQ, T> bt)
@@ -870,7 +882,7 @@ __global__ void k_dz(Batch<NQ, T> bt)
 // zero iterations is converged; the batch is done once the converged count
 // reaches B * solve_ratio.
 template <int NQ, typename T>
-__global__ void k_check(Batch<NQ, T> bt)
+__device__ __forceinline__ void check_body(const Batch<NQ, T>& bt)
 {
     __shared__ int s_count;
     if (threadIdx.x == 0) s_count = 0;
@@ -895,6 +907,12 @@ __global__ void k_check(Batch<NQ, T> bt)
         if ((float)s_count >= (float)bt.B * bt.solve_ratio) *bt.done = 1;
         else *bt.ls_count += 1;
     }
+}
+
+template <int NQ, typename T>
+__global__ void k_check(Batch<NQ, T> bt)
+{
+    check_body<NQ, T>(bt);
 }
 
 // Shared memory of the fused SQP-iteration kernel.
@@ -931,23 +949,51 @@ struct FusedLayout {
 // complement, PCG, step recovery), one block.  With with_pcg = 0 it stops
 // after the Schur complement (S, P^-1 and gamma left in global memory) and
 // k_pcg_rows takes over.
-template <int NQ, typename T, typename Acc>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int it_row,
-                             int with_pcg)
+// A group of consecutive warps of a CTA that works on one problem, with its
+// own barrier: the whole CTA (barrier 0, __syncthreads) or a fixed slice of
+// it synchronised by a named barrier.
+struct Team {
+    int tid, nthreads, warp, nwarps, bar;
+    __device__ static Team cta()
+    {
+        return Team{(int)threadIdx.x, (int)blockDim.x, warp_id(), (int)(blockDim.x / WARP), 0};
+    }
+    // slice t of `count` equal slices of the CTA
+    __device__ static Team slice(int t, int count)
+    {
+        const int nt = blockDim.x / count;
+        return Team{(int)threadIdx.x - t * nt, nt, warp_id() - t * (nt / WARP), nt / WARP, 1 + t};
+    }
+    __device__ __forceinline__ void sync() const
+    {
+        if (bar == 0)
+            __syncthreads();
+        else
+            asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nthreads) : "memory");
+    }
+};
+
+// KG: lanes per knot in the KKT stage (16: two knots per warp, 32: one).
+// `team` is the set of warps working on this problem (the whole CTA, or half
+// of it when a CTA runs two problems at once); with_pcg needs the whole CTA.
+template <int NQ, typename T, typename Acc, int KG = 16>
+__device__ __forceinline__ void fused_iter_body(const Batch<NQ, T>& bt, const DevModel<NQ, T>& M,
+                                                int b, int stage, int it_row, int with_pcg,
+                                                unsigned char* smem_raw,
+                                                const Team& team = Team::cta())
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
     if (*bt.done) return;
-    const int b = blockIdx.x;
     const int N = bt.N;
     const Dims<NQ> d{N};
     constexpr int nx = Dims<NQ>::nx, nu = Dims<NQ>::nu;
-    const int nw = blockDim.x / WARP;
+    const int nw = team.nwarps;
+    const int wid = team.warp;
     FusedLayout<NQ, T> lay{N, nw, stage != 0};
     T* mats = smem;
     T* work = smem + lay.mats_floats();
     const size_t sc = lay.scratch_floats() / nw;
-    T* ws = work + warp_id() * sc;
+    T* ws = work + wid * sc;
     size_t wfl = lay.scratch_floats() > lay.vec_floats() ? lay.scratch_floats() : lay.vec_floats();
     Acc* red = reinterpret_cast<Acc*>(((uintptr_t)(work + wfl) + 15) & ~(uintptr_t)15);
 
@@ -967,11 +1013,16 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_fused_iter(Batc
     const T* xu = bt.xu + (size_t)b * d.traj();
     const T* fext = bt.use_fext ? bt.fext + 6 * b : nullptr;
 
-    // KKT set-up, two knots per warp (one per half-warp)
-    {
+    // KKT set-up, two knots per warp (one per half-warp) or one per warp
+    if constexpr (KG == 32) {
+        for (int k = wid; k < N - 1; k += nw)
+            kkt_knot<NQ, T, 32>(M, cost_of<NQ>(bt.cp, b), N, k, xu, bt.xs + (size_t)b * nx,
+                                bt.goal + (size_t)b * d.goal(), fext, Q, R, qv, rv, A, Bm, c,
+                                ws, true);
+    } else {
         const int half = lane_id() >> 4;
         const int npairs = N / 2;  // ceil((N - 1) / 2)
-        for (int kp = warp_id(); kp < npairs; kp += nw) {
+        for (int kp = wid; kp < npairs; kp += nw) {
             const int k = 2 * kp + half;
             const bool valid = k < N - 1;
             kkt_knot<NQ, T, 16>(M, cost_of<NQ>(bt.cp, b), N, valid ? k : N - 2, xu, bt.xs + (size_t)b * nx,
@@ -979,14 +1030,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_fused_iter(Batc
                                 ws + half * KktSmem<NQ>::SIZE, valid);
         }
     }
-    __syncthreads();
-    for (int k = warp_id(); k < N; k += nw) {
+    team.sync();
+    for (int k = wid; k < N; k += nw) {
         warp_invert<nx, T>(Q + k * nx * nx, rho, Qi + k * nx * nx);
         if (k < N - 1) warp_invert<nu, T>(R + k * nu * nu, T(0), Ri + k * nu * nu);
     }
     if (stage) {
         // the padding blocks of S and P^-1 (row 0 left, row N-1 right) are zero
-        for (int i = threadIdx.x; i < nx * 3 * nx; i += blockDim.x) {
+        for (int i = team.tid; i < nx * 3 * nx; i += team.nthreads) {
             const int y = i / (3 * nx), x = i % (3 * nx);
             if (x < nx) {
                 S[y * 3 * nx + x] = 0.0f;
@@ -997,29 +1048,37 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_fused_iter(Batc
             }
         }
     }
-    __syncthreads();
-    for (int k = warp_id(); k < N; k += nw) {
+    team.sync();
+    for (int k = wid; k < N; k += nw) {
         if (k == N - 1)
             schur_first<NQ, T>(rho, Q, Qi, qv, c, S, P, g);
         else
             schur_knot<NQ, T>(k, rho, Qi, Ri, qv, rv, A, Bm, c, S, P, g, ws);
     }
-    __syncthreads();
-    for (int k = warp_id(); k < N - 1; k += nw) schur_offdiag<NQ, T>(k, S, P, ws);
+    team.sync();
+    for (int k = wid; k < N - 1; k += nw) schur_offdiag<NQ, T>(k, S, P, ws);
     if (!with_pcg) return;  // k_pcg_rows continues from S, P^-1 in global memory
-    __syncthreads();
+    team.sync();
     int iters = 0;
     if (!bt.conv[b])
         iters = pcg_block<NQ, T, Acc>(N, S, P, g, bt.lambda + (size_t)b * d.vecp(), bt.tol[b],
                                    bt.max_pcg_iters, work, red, bt.abs_tol);
-    __syncthreads();
-    for (int k = warp_id(); k < N; k += nw)
+    team.sync();
+    for (int k = wid; k < N; k += nw)
         dz_knot<NQ, T>(N, k, bt.lambda + (size_t)b * d.vecp(), Qi, Ri, qv, rv, A, Bm,
                     bt.dz + (size_t)b * d.traj(), ws);
-    if (threadIdx.x == 0) {
+    if (team.tid == 0) {
         bt.pcg_iters[b] = iters;
         if (bt.h_pcg) bt.h_pcg[(size_t)it_row * bt.B + b] = iters;
     }
+}
+
+template <int NQ, typename T, typename Acc>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+    k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int it_row, int with_pcg)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    fused_iter_body<NQ, T, Acc>(bt, M, blockIdx.x, stage, it_row, with_pcg, smem_raw);
 }
 
 }  // namespace gato

@@ -49,6 +49,7 @@ class BSQP:
         form="fused",
         precision="fp32",
         model=None,
+        _handle=None,
     ):
         if plant_type is None:
             plant_type = "iiwa14" if (model_path and "iiwa" in model_path.lower()) else "indy7"
@@ -65,12 +66,16 @@ class BSQP:
         if precision not in L.PRECISIONS:
             raise ValueError(f"unknown precision {precision!r}")
         h = ctypes.c_void_p()
-        try:
-            L.check(lib.gato_create(ctypes.byref(self._model), int(N), int(batch_size),
-                                    ctypes.byref(self.params), L.FORMS[form],
-                                    L.PRECISIONS[precision], ctypes.byref(h)))
-        except L.GatoError as e:
-            raise ValueError(str(e)) from e
+        self._owned = _handle is None
+        if _handle is not None:  # a solver owned by a mixed batch (gato_mixed_class)
+            h = _handle
+        else:
+            try:
+                L.check(lib.gato_create(ctypes.byref(self._model), int(N), int(batch_size),
+                                        ctypes.byref(self.params), L.FORMS[form],
+                                        L.PRECISIONS[precision], ctypes.byref(h)))
+            except L.GatoError as e:
+                raise ValueError(str(e)) from e
         self._h = h
         self.batch_size = int(batch_size)
         self.N = int(N)
@@ -107,7 +112,8 @@ class BSQP:
     # -- lifetime ---------------------------------------------------------
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
-            L.load().gato_destroy(self._h)
+            if getattr(self, "_owned", True):
+                L.load().gato_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

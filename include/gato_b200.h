@@ -323,6 +323,48 @@ int gato_pcg_static(void* stream, int nq, int N, int batch, float pcg_tol,
                     int max_pcg_iters, const float* d_S, const float* d_Pinv,
                     const float* d_gamma, float* d_lambda, int32_t* d_iters);
 
+/* ---- Mixed batches (no counterpart in the reference, which builds one
+   module per plant and horizon and one class per power-of-two batch; a mixed
+   workload there is one call per module).  Problems are grouped into classes
+   (plant, N, count); each class is an ordinary fused-form solver (buffers,
+   lambda, rho, setters: gato_mixed_class), and every stage of an SQP
+   iteration runs as ONE persistent launch over all classes that takes
+   problems from a device work queue, longest horizon first; long horizons
+   take the cluster PCG on a parallel branch.  The whole solve is one CUDA
+   graph.  All classes share the parameters and precision. */
+typedef struct {
+    int plant; /* GATO_PLANT_* */
+    int N;     /* knots */
+    int count; /* problems of this class */
+} gato_class_t;
+typedef struct gato_mixed gato_mixed_t;
+
+int gato_mixed_create(const gato_class_t* classes, int nclasses,
+                      const gato_params_t* params, int precision,
+                      gato_mixed_t** out);
+int gato_mixed_destroy(gato_mixed_t* mx);
+/* the solver of class c (owned by mx): setters, lambda, rho, stats buffers */
+int gato_mixed_class(gato_mixed_t* mx, int c, gato_solver_t** out);
+/* d_xu / d_xs / d_goal: host arrays of nclasses device pointers (the
+   solver scalar type), laid out per class as for gato_solve. */
+int gato_mixed_solve(gato_mixed_t* mx, void* stream, void* const* d_xu,
+                     const void* const* d_xs, const void* const* d_goal);
+/* per-class statistics of the last solve (waits for it) */
+int gato_mixed_stats(gato_mixed_t* mx, int c, gato_stats_t* stats);
+/* device time of the last solve in ms (waits for it) */
+int gato_mixed_elapsed_ms(gato_mixed_t* mx, float* ms);
+/* KKT-stage launch shape: lanes per knot (16: two knots per warp, 32: one)
+   and problems per CTA (1 or 2) */
+int gato_mixed_config(gato_mixed_t* mx, int lanes_per_knot,
+                      int problems_per_block);
+/* Autotuner: times the solve of these inputs under each launch shape
+   (lanes per knot x problems per CTA, in the order (16,1) (16,2) (32,1)
+   (32,2), ms_out[4] optional), restores XU, lambda, rho and drho after every
+   trial, and keeps the fastest shape.  Allocates temporary copies. */
+int gato_mixed_tune(gato_mixed_t* mx, void* stream, void* const* d_xu,
+                    const void* const* d_xs, const void* const* d_goal,
+                    float* ms_out);
+
 #ifdef __cplusplus
 }
 #endif
