@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="problems in the CPU baseline sample (0: sized to ~10 s)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", default="single", choices=["single", "mixed"],
+                    help="single: the headline iiwa14 N=32 batch; mixed: 4096 problems of "
+                         "both plants and four horizons in one solve")
     return ap.parse_args()
 
 
@@ -599,8 +602,193 @@ def run_ours(args):
     return 0
 
 
+# --------------------------------------------------------------------------
+# mixed workload: 4096 problems, plant 50/50 indy7 / iiwa14, horizon drawn
+# from {8, 32, 64, 128}, figure-8 goals, default warm start, per-problem rho
+# ~ logU[1e-2, 1e2], FP32 arithmetic with FP64 PCG inner products and merit
+# sums, 5 SQP iterations, PCG max 173 at tol 1e-5
+MIXED_TOTAL, MIXED_HORIZONS, MIXED_PLANTS = 4096, (8, 32, 64, 128), ("indy7", "iiwa14")
+
+
+def mixed_classes(seed=2027):
+    """(plant, N, count) of the seeded draw, longest first, and per-class
+    seeds for the problem data."""
+    rng = np.random.default_rng(seed)
+    plants = rng.integers(0, 2, MIXED_TOTAL)
+    hor = rng.integers(0, 4, MIXED_TOTAL)
+    out = []
+    for h in reversed(range(4)):
+        for p in (1, 0):
+            c = int(np.sum((plants == p) & (hor == h)))
+            if c:
+                out.append((MIXED_PLANTS[p], MIXED_HORIZONS[h], c))
+    return out
+
+
+def mixed_data(classes, seed=2027):
+    from gato_b200 import workloads as W
+    rng = np.random.default_rng(seed + 1)
+    data = []
+    for i, (plant, n, c) in enumerate(classes):
+        pr = W.make_problem(plant, n, c, seed=seed + 10 + i, goals="figure8", dt=DT)
+        pr["rho"] = np.exp(rng.uniform(np.log(1e-2), np.log(1e2), c)).astype(np.float32)
+        data.append(pr)
+    return data
+
+
+def mixed_kwargs():
+    kw = solver_kwargs()
+    return kw
+
+
+def run_mixed(args):
+    import torch
+    import gato_b200
+    from gato_b200.mixed import MixedBSQP
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda")
+    classes = mixed_classes()
+    data = mixed_data(classes)
+    kw = mixed_kwargs()
+    T = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
+    xs = [T(d["xs"]) for d in data]
+    goal = [T(d["goal"]) for d in data]
+    xu0 = [T(d["xu"]) for d in data]
+    xu = [x.clone() for x in xu0]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    mx = MixedBSQP(classes, dt=DT, precision="mixed", **kw)
+
+    def reset(solvers, ds=None):
+        for s, d in zip(solvers, ds or data):
+            s.set_rho_penalty_batch(d["rho"], True)
+            s.reset_dual()
+            s.reset_rho()
+
+    reset(mx.cls)
+    with torch.cuda.stream(stream):
+        shapes = mx.tune(xu, xs, goal, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    times = []
+    for i in range(args.warmup + args.steps):
+        for a, b in zip(xu, xu0):
+            a.copy_(b)
+        reset(mx.cls)
+        flush.zero_()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            mx.solve_device(xu, xs, goal, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            times.append(mx.elapsed_ms())
+    stats = [mx.stats(c) for c in range(len(classes))]
+    mx.close()
+    # each class alone in its own fused solver (graph), one after another:
+    # how a caller of per-(plant, N) solvers runs this workload
+    alone = []
+    for (plant, n, c), d, x0, xsc, gc in zip(classes, data, xu0, xs, goal):
+        s = gato_b200.BSQP(batch_size=c, N=n, dt=DT, plant_type=plant, precision="mixed",
+                           form="fused", **kw)
+        x = x0.clone()
+        ts = []
+        for i in range(args.warmup + max(3, args.steps // 2)):
+            x.copy_(x0)
+            reset([s], [d])
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                s.solve_device(x, xsc, gc, stream=stream.cuda_stream, with_stats=False)
+                e1.record(stream)
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                ts.append(e0.elapsed_time(e1))
+        s.close()
+        alone.append(float(np.median(ts)))
+    ms = float(np.mean(times))
+    line = {
+        "metric": "mixed-batch SQP solves/s (4096 problems: indy7/iiwa14 x N 8/32/64/128)",
+        "value": MIXED_TOTAL / (ms * 1e-3), "unit": "solves/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "p50_ms": float(np.median(times)), "p99_ms": float(np.percentile(times, 99)),
+        "higher_is_better": True, "dtype": "f32+f64-reductions",
+        "data": "synthetic (seeded draw of plants/horizons, figure-8 goals, rho ~ logU[1e-2,1e2])",
+        "config": {"workload": "mixed 4096", "classes": classes, "sqp_iters": SQP_ITERS,
+                   "l2": "flushed between steps"},
+        "tuner_ms": {f"lanes{k[0]}_ppb{k[1]}": v for k, v in shapes.items()},
+        "per_class": [{"plant": p, "N": n, "count": c, "alone_ms": a,
+                       "pcg_iters_mean": float(np.mean(st["pcg_iters"]))}
+                      for (p, n, c), a, st in zip(classes, alone, stats)],
+        "sequential_alone_ms": float(sum(alone)),
+        "mixed_vs_sequential": float(sum(alone)) / ms,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_reference_mixed(args):
+    """The reference's own CUDA modules (one per plant and horizon, built by
+    oracle/build_ref_gpu.py) on the mixed workload, as its interface runs it:
+    one solve() per class, the batch padded to the next power of two."""
+    import glob
+    import importlib.util
+    classes = mixed_classes()
+    data = mixed_data(classes)
+    kw = mixed_kwargs()
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError
+    except Exception:
+        print(json.dumps({"impl": "reference", "unavailable": "no GPU"}))
+        return 0
+    per = []
+    for (plant, n, c), d in zip(classes, data):
+        paths = glob.glob(os.path.join(ROOT, "oracle", "_ref", f"bsqpN{n}_{plant}*.so"))
+        if not paths:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              f"reference module bsqpN{n}_{plant} not built "
+                              f"(oracle/build_ref_gpu.py {plant}:{n})"}))
+            return 0
+        spec = importlib.util.spec_from_file_location(f"bsqpN{n}_{plant}", paths[0])
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        bp = 1 << max(0, (c - 1).bit_length())
+        cls = getattr(mod, f"BSQP_{bp}_float")
+        solver = cls(DT, kw["max_sqp_iters"], kw["kkt_tol"], kw["max_pcg_iters"], kw["pcg_tol"],
+                     kw["solve_ratio"], kw["mu"], kw["q_cost"], kw["qd_cost"], kw["u_cost"],
+                     kw["N_cost"], kw["q_lim_cost"], kw["vel_lim_cost"], kw["ctrl_lim_cost"],
+                     kw["rho"])
+        pad = lambda a: np.ascontiguousarray(np.concatenate(
+            [a, np.repeat(a[-1:], bp - c, axis=0)]), dtype=np.float32)
+        xu, xs, goal, rho = pad(d["xu"]), pad(d["xs"]), pad(d["goal"]), pad(d["rho"])
+        ts = []
+        for i in range(args.warmup + max(3, args.steps // 2)):
+            solver.set_rho_penalty_batch(rho, True)
+            solver.reset_dual()
+            solver.reset_rho()
+            x = xu.copy()
+            t0 = time.perf_counter()
+            solver.solve(x, DT, xs, goal)
+            t1 = time.perf_counter()
+            if i >= args.warmup:
+                ts.append(1e3 * (t1 - t0))
+        per.append({"plant": plant, "N": n, "count": c, "padded_batch": bp,
+                    "ms": float(np.median(ts))})
+        del solver
+    total = sum(p["ms"] for p in per)
+    print(json.dumps({"impl": "reference", "metric": "mixed-batch SQP solves/s",
+                      "value": MIXED_TOTAL / (total * 1e-3), "unit": "solves/s",
+                      "ms_per_step": total, "higher_is_better": True, "per_class": per,
+                      "kind": "reference CUDA modules, one solve() per class (host arrays)"}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "mixed":
+        return run_reference_mixed(args) if args.impl == "reference" else run_mixed(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
