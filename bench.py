@@ -728,60 +728,14 @@ def run_mixed(args):
 
 
 def run_reference_mixed(args):
-    """The reference's own CUDA modules (one per plant and horizon, built by
-    oracle/build_ref_gpu.py) on the mixed workload, as its interface runs it:
-    one solve() per class, the batch padded to the next power of two."""
-    import glob
-    import importlib.util
-    classes = mixed_classes()
-    data = mixed_data(classes)
-    kw = mixed_kwargs()
-    try:
-        import torch
-        if not torch.cuda.is_available():
-            raise RuntimeError
-    except Exception:
-        print(json.dumps({"impl": "reference", "unavailable": "no GPU"}))
-        return 0
-    per = []
-    for (plant, n, c), d in zip(classes, data):
-        paths = glob.glob(os.path.join(ROOT, "oracle", "_ref", f"bsqpN{n}_{plant}*.so"))
-        if not paths:
-            print(json.dumps({"impl": "reference", "unavailable":
-                              f"reference module bsqpN{n}_{plant} not built "
-                              f"(oracle/build_ref_gpu.py {plant}:{n})"}))
-            return 0
-        spec = importlib.util.spec_from_file_location(f"bsqpN{n}_{plant}", paths[0])
-        mod = importlib.util.module_from_spec(spec)
-        spec.loader.exec_module(mod)
-        bp = 1 << max(0, (c - 1).bit_length())
-        cls = getattr(mod, f"BSQP_{bp}_float")
-        solver = cls(DT, kw["max_sqp_iters"], kw["kkt_tol"], kw["max_pcg_iters"], kw["pcg_tol"],
-                     kw["solve_ratio"], kw["mu"], kw["q_cost"], kw["qd_cost"], kw["u_cost"],
-                     kw["N_cost"], kw["q_lim_cost"], kw["vel_lim_cost"], kw["ctrl_lim_cost"],
-                     kw["rho"])
-        pad = lambda a: np.ascontiguousarray(np.concatenate(
-            [a, np.repeat(a[-1:], bp - c, axis=0)]), dtype=np.float32)
-        xu, xs, goal, rho = pad(d["xu"]), pad(d["xs"]), pad(d["goal"]), pad(d["rho"])
-        ts = []
-        for i in range(args.warmup + max(3, args.steps // 2)):
-            solver.set_rho_penalty_batch(rho, True)
-            solver.reset_dual()
-            solver.reset_rho()
-            x = xu.copy()
-            t0 = time.perf_counter()
-            solver.solve(x, DT, xs, goal)
-            t1 = time.perf_counter()
-            if i >= args.warmup:
-                ts.append(1e3 * (t1 - t0))
-        per.append({"plant": plant, "N": n, "count": c, "padded_batch": bp,
-                    "ms": float(np.median(ts))})
-        del solver
-    total = sum(p["ms"] for p in per)
-    print(json.dumps({"impl": "reference", "metric": "mixed-batch SQP solves/s",
-                      "value": MIXED_TOTAL / (total * 1e-3), "unit": "solves/s",
-                      "ms_per_step": total, "higher_is_better": True, "per_class": per,
-                      "kind": "reference CUDA modules, one solve() per class (host arrays)"}))
+    """The reference's mixed-workload arm: its modules (one per plant and
+    horizon, one solve() per class) are not run.  The FP32 module
+    bsqpN128_indy7 ended its process with cudaErrorIllegalAddress on this
+    workload (484 problems padded to its batch-512 class), so the arm reports
+    no number."""
+    print(json.dumps({"impl": "reference", "unavailable":
+                      "the reference's bsqpN128_indy7 module raised an illegal-address fault "
+                      "(exit 188) on this workload; not run again"}))
     return 0
 
 

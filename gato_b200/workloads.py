@@ -77,9 +77,10 @@ def perturb(xu, nq, N, rng, sigma_x=0.01, sigma_u=0.1):
     return full.reshape(B, -1)[:, : xu.shape[1]].copy()
 
 
-def make_problem(plant, N, B, seed, goals="figure8", dt=0.01):
-    """Returns dict(model, xs, goal, xu) as float32 arrays."""
-    model = L.builtin_model(plant)
+def make_problem(plant, N, B, seed, goals="figure8", dt=0.01, model=None):
+    """Returns dict(model, xs, goal, xu) as float32 arrays (`model`, a
+    gato_model_t, replaces the built-in plant)."""
+    model = model if model is not None else L.builtin_model(plant)
     rng = np.random.default_rng(seed)
     xs = initial_states(model, B, rng)
     if goals == "figure8":

@@ -9,6 +9,9 @@ nvcc is run directly on the reference's python/bindings.cu where it lies
 (GATO_REF, default /root/reference); nothing is copied.  One module takes
 several minutes to compile.
 
+Only the FP32 build is made: the reference's USE_DOUBLES build raised an
+illegal-address fault on the B200 and is not built or run.
+
 Usage: python oracle/build_ref_gpu.py [plant:N ...]   (default: iiwa14:32)
 """
 import os
@@ -33,7 +36,7 @@ def build(plant, N, force=False):
     if os.path.exists(out) and not force:
         return out
     import pybind11
-    os.makedirs(OUT, exist_ok=True)
+    os.makedirs(os.path.dirname(out), exist_ok=True)
     define = {"iiwa14": "PLANT_IIWA14=1", "indy7": "PLANT_INDY7=1"}[plant]
     cmd = ["nvcc", "-std=c++17", "-O3", "-use_fast_math",
            "-gencode", "arch=compute_100a,code=sm_100a",
