@@ -116,6 +116,10 @@ SIGNATURES = {
     "gato_stage_form_schur": (ctypes.c_int, [_vp, _vp] + [_vp] * 10),
     "gato_stage_pcg": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gato_set_cost_diag_batch": (ctypes.c_int, [_vp, _vp]),
+    "gato_rollout": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "gato_rollout_backward": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp,
+                                             _vp, _vp, _vp, _vp, ctypes.c_double,
+                                             ctypes.c_int]),
     "gato_mixed_create": (ctypes.c_int, [ctypes.POINTER(GatoClass), ctypes.c_int,
                                          ctypes.POINTER(GatoParams), ctypes.c_int,
                                          ctypes.POINTER(_vp)]),

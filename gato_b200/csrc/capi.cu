@@ -18,6 +18,7 @@
 #include "kernels.cuh"
 #include "multi.cuh"
 #include "pcg_cluster.cuh"
+#include "rollout.cuh"
 #include "plant_tables.h"
 
 using namespace gato;
@@ -191,6 +192,13 @@ struct gato_solver {
     void *adj_lam = nullptr, *adj_mu = nullptr, *adj_v = nullptr, *adj_scale = nullptr,
          *adj_tol = nullptr;
     int *adj_conv = nullptr, *adj_done = nullptr, *adj_iters = nullptr;
+    // rollout work buffers, allocated by the first gato_rollout* call
+    void *rl_goal = nullptr, *rl_gx = nullptr, *rl_ga = nullptr, *rl_gu = nullptr,
+         *rl_dl = nullptr, *rl_gxs = nullptr, *rl_ggoal = nullptr, *rl_gw = nullptr,
+         *rl_rho = nullptr;
+    cudaGraphExec_t rexec = nullptr;  // forward rollout graph
+    std::vector<const void*> rkey;
+    int rver = -1;
     // host
     std::vector<double> rho_init, drho_init;
     int* pin_i = nullptr;  // pinned host ints (B)
@@ -830,6 +838,131 @@ int adjoint_impl(gato_solver* s, cudaStream_t st, void* xu, const void* xs, cons
     return GATO_OK;
 }
 
+// --- closed-loop rollout ---------------------------------------------------------
+int rollout_alloc(gato_solver* s)
+{
+    if (s->rl_rho) return GATO_OK;
+    const size_t B = s->B, nx = 2 * s->nq, nu = s->nq, N = s->N;
+    const size_t traj = (nx + nu) * N - nu;
+    RC(s->alloc_t(&s->rl_goal, B * 6 * N));
+    RC(s->alloc_t(&s->rl_gx, B * nx));
+    RC(s->alloc_t(&s->rl_ga, B * nx));
+    RC(s->alloc_t(&s->rl_gu, B * nu));
+    RC(s->alloc_t(&s->rl_dl, B * traj));
+    RC(s->alloc_t(&s->rl_gxs, B * nx));
+    RC(s->alloc_t(&s->rl_ggoal, B * 6 * N));
+    RC(s->alloc_t(&s->rl_gw, B * (nx + nu)));
+    RC(s->alloc_t(&s->rl_rho, B));  // last: it marks the set as complete
+    return GATO_OK;
+}
+
+template <class Tg>
+int enqueue_rollout(gato_solver* s, cudaStream_t st, int steps, const void* goal_traj, void* xu,
+                    const void* noise, void* x, void* u, void* ckpt_xu, void* ckpt_rho)
+{
+    constexpr int NQ = Tg::NQ;
+    using T = typename Tg::T;
+    const int B = s->B, N = s->N, nx = 2 * NQ, nu = NQ;
+    const int traj = (nx + nu) * N - nu, stride = 6 * (N + steps);
+    const size_t smem_sim = WPB * (DynSmem<NQ>::SIZE + 3 * NQ) * sizeof(T);
+    for (int t = 0; t < steps; ++t) {
+        T* xt = (T*)x + (size_t)t * B * nx;
+        k_goal_window<T><<<cdiv(B * 6 * N, 256), 256, 0, st>>>((const T*)goal_traj, stride, t, N,
+                                                                B, (T*)s->rl_goal);
+        CKL();
+        k_set_x0<T><<<cdiv(B * nx, 256), 256, 0, st>>>((T*)xu, xt, B, traj, nx);
+        CKL();
+        RC(enqueue_fused<Tg>(s, st, xu, xt, s->rl_goal));
+        if (ckpt_xu)
+            CK(cudaMemcpyAsync((T*)ckpt_xu + (size_t)t * B * traj, xu, sizeof(T) * B * traj,
+                               cudaMemcpyDeviceToDevice, st));
+        if (ckpt_rho)
+            CK(cudaMemcpyAsync((T*)ckpt_rho + (size_t)t * B, s->rho, sizeof(T) * B,
+                               cudaMemcpyDeviceToDevice, st));
+        k_sim_step<NQ, T><<<cdiv(B, WPB), WPB * WARP, smem_sim, st>>>(
+            dmodel<Tg>(s), B, (T)s->dt, xt, (const T*)xu, traj,
+            noise ? (const T*)noise + (size_t)t * B * nu : nullptr, (const T*)s->fext,
+            s->use_fext, xt + (size_t)B * nx, (T*)u + (size_t)t * B * nu);
+        CKL();
+        k_shift<T><<<B, 128, sizeof(T) * traj, st>>>((T*)xu, xt + (size_t)B * nx, N, nx, nu);
+        CKL();
+    }
+    return GATO_OK;
+}
+
+template <class Tg>
+int enqueue_rollout_backward(gato_solver* s, cudaStream_t st, int steps, const void* goal_traj,
+                             const void* x, const void* u, const void* ckpt_xu,
+                             const void* ckpt_rho, const void* dl_dx, void* g_x0, void* g_goal,
+                             void* g_wdiag, double tol, int max_iters)
+{
+    constexpr int NQ = Tg::NQ;
+    using T = typename Tg::T;
+    const int B = s->B, N = s->N, nx = 2 * NQ, nu = NQ;
+    const int traj = (nx + nu) * N - nu, stride = 6 * (N + steps);
+    const size_t smem_vjp = WPB * (DynSmem<NQ>::SIZE + 3 * NQ + nx) * sizeof(T);
+    CK(cudaMemcpyAsync(s->rl_rho, s->rho, sizeof(T) * B, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s->rl_gx, (const T*)dl_dx + (size_t)steps * B * nx, sizeof(T) * B * nx,
+                       cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemsetAsync(g_goal, 0, sizeof(T) * (size_t)B * stride, st));
+    CK(cudaMemsetAsync(g_wdiag, 0, sizeof(T) * (size_t)B * (nx + nu), st));
+    for (int t = steps - 1; t >= 0; --t) {
+        const T* xt = (const T*)x + (size_t)t * B * nx;
+        k_sim_vjp<NQ, T><<<cdiv(B, WPB), WPB * WARP, smem_vjp, st>>>(
+            dmodel<Tg>(s), B, (T)s->dt, xt, (const T*)u + (size_t)t * B * nu,
+            (const T*)s->rl_gx, (const T*)s->fext, s->use_fext, (T*)s->rl_ga, (T*)s->rl_gu);
+        CKL();
+        k_scatter_u0<T><<<cdiv(B * traj, 256), 256, 0, st>>>((T*)s->rl_dl, (const T*)s->rl_gu, B,
+                                                           traj, nx, nu);
+        CKL();
+        CK(cudaMemcpyAsync(s->rho, (const T*)ckpt_rho + (size_t)t * B, sizeof(T) * B,
+                           cudaMemcpyDeviceToDevice, st));
+        k_goal_window<T><<<cdiv(B * 6 * N, 256), 256, 0, st>>>((const T*)goal_traj, stride, t, N,
+                                                                B, (T*)s->rl_goal);
+        CKL();
+        RC(adjoint_impl<Tg>(s, st, (void*)((const T*)ckpt_xu + (size_t)t * B * traj), xt,
+                            s->rl_goal, s->rl_dl, s->rl_gxs, s->rl_ggoal, s->rl_gw, tol,
+                            max_iters, nullptr));
+        CK(cudaMemcpyAsync(s->rl_gx, (const T*)dl_dx + (size_t)t * B * nx, sizeof(T) * B * nx,
+                           cudaMemcpyDeviceToDevice, st));
+        k_add3<T><<<cdiv(B * nx, 256), 256, 0, st>>>((T*)s->rl_gx, (const T*)s->rl_ga,
+                                                   (const T*)s->rl_gxs, B * nx);
+        CKL();
+        k_accum<T><<<cdiv(B * (nx + nu), 256), 256, 0, st>>>((T*)g_wdiag, (const T*)s->rl_gw,
+                                                            B * (nx + nu));
+        CKL();
+        k_goal_accum<T><<<cdiv(B * 6 * N, 256), 256, 0, st>>>((T*)g_goal, (const T*)s->rl_ggoal,
+                                                               stride, t, N, B);
+        CKL();
+    }
+    CK(cudaMemcpyAsync(g_x0, s->rl_gx, sizeof(T) * B * nx, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s->rho, s->rl_rho, sizeof(T) * B, cudaMemcpyDeviceToDevice, st));
+    return GATO_OK;
+}
+
+// captures `enqueue` into a graph on a private stream and launches it on st
+template <class F>
+int capture_and_launch(cudaStream_t st, F&& enqueue, cudaGraphExec_t* exec)
+{
+    cudaStream_t cap;
+    CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue(cap);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(cap, &graph);
+    cudaStreamDestroy(cap);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(GATO_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(GATO_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    CK(cudaGraphLaunch(*exec, st));
+    return GATO_OK;
+}
+
 // sim_forward: one warp per problem (simForwardBatchedKernel,
 // gato/bsqp/kernels/sim.cuh:14-49).
 template <int NQ, typename T>
@@ -1048,6 +1181,7 @@ void gato_destroy(gato_solver_t* s)
     cudaGetDevice(&cur);
     cudaSetDevice(s->device);
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
+    if (s->rexec) cudaGraphExecDestroy(s->rexec);
     for (void* v : s->allocs) cudaFree(v);
     if (s->pin_i) cudaFreeHost(s->pin_i);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
@@ -1444,6 +1578,72 @@ int gato_adjoint_f64(gato_solver_t* s, void* stream, const double* d_xu, const d
                                           d_dl_dxu, d_g_xs, d_g_goal, d_g_wdiag, tol, max_iters,
                                           h_iters);
     });
+}
+
+int gato_rollout(gato_solver_t* s, void* stream, int steps, const void* d_goal_traj, void* d_xu,
+                 const void* d_noise, void* d_x, void* d_u, void* d_ckpt_xu, void* d_ckpt_rho)
+{
+    RC(check_handle(s));
+    if (s->form != GATO_FORM_FUSED) return fail(GATO_ERR_UNSUPPORTED, "rollout needs the fused form");
+    if (steps < 1) return fail(GATO_ERR_ARG, "steps must be positive");
+    if (!d_goal_traj || !d_xu || !d_x || !d_u) return fail(GATO_ERR_ARG, "null device buffer");
+    RC(bind_device(s));
+    RC(rollout_alloc(s));
+    cudaStream_t st = as_stream(stream);
+    std::vector<const void*> key = {d_goal_traj, d_xu, d_noise, d_x, d_u, d_ckpt_xu, d_ckpt_rho,
+                                    (const void*)st, (const void*)(intptr_t)steps};
+    if (s->rexec && key == s->rkey && s->rver == s->version) {
+        CK(cudaGraphLaunch(s->rexec, st));
+        return GATO_OK;
+    }
+    if (s->rexec) {
+        cudaGraphExecDestroy(s->rexec);
+        s->rexec = nullptr;
+    }
+    RC(dispatch(s, [&](auto tg) {
+        using Tg = decltype(tg);
+        return capture_and_launch(st, [&](cudaStream_t cap) {
+            return enqueue_rollout<Tg>(s, cap, steps, d_goal_traj, d_xu, d_noise, d_x, d_u,
+                                       d_ckpt_xu, d_ckpt_rho);
+        }, &s->rexec);
+    }));
+    s->rkey = key;
+    s->rver = s->version;
+    return GATO_OK;
+}
+
+int gato_rollout_backward(gato_solver_t* s, void* stream, int steps, const void* d_goal_traj,
+                          const void* d_x, const void* d_u, const void* d_ckpt_xu,
+                          const void* d_ckpt_rho, const void* d_dl_dx, void* d_g_x0,
+                          void* d_g_goal_traj, void* d_g_wdiag, double tol, int max_iters)
+{
+    RC(check_handle(s));
+    if (s->form != GATO_FORM_FUSED) return fail(GATO_ERR_UNSUPPORTED, "rollout needs the fused form");
+    if (steps < 1) return fail(GATO_ERR_ARG, "steps must be positive");
+    if (!d_goal_traj || !d_x || !d_u || !d_ckpt_xu || !d_ckpt_rho || !d_dl_dx || !d_g_x0 ||
+        !d_g_goal_traj || !d_g_wdiag)
+        return fail(GATO_ERR_ARG, "null device buffer");
+    RC(bind_device(s));
+    RC(rollout_alloc(s));
+    RC(adj_alloc(s));
+    const bool f64 = s->precision == GATO_PREC_FP64;
+    if (tol <= 0) tol = f64 ? 1e-20 : 1e-12;
+    if (max_iters <= 0) max_iters = 4 * s->N * s->nq;
+    cudaStream_t st = as_stream(stream);
+    cudaGraphExec_t exec = nullptr;
+    int rc = dispatch(s, [&](auto tg) {
+        using Tg = decltype(tg);
+        return capture_and_launch(st, [&](cudaStream_t cap) {
+            return enqueue_rollout_backward<Tg>(s, cap, steps, d_goal_traj, d_x, d_u, d_ckpt_xu,
+                                                d_ckpt_rho, d_dl_dx, d_g_x0, d_g_goal_traj,
+                                                d_g_wdiag, tol, max_iters);
+        }, &exec);
+    });
+    if (exec) {
+        cudaStreamSynchronize(st);
+        cudaGraphExecDestroy(exec);
+    }
+    return rc;
 }
 
 }  // extern "C"

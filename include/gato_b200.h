@@ -302,6 +302,35 @@ int gato_adjoint_f64(gato_solver_t* s, void* stream, const double* d_xu,
                      double* d_g_wdiag, double tol, int max_iters,
                      int32_t* h_iters);
 
+/* Closed-loop receding-horizon rollout (no counterpart in the reference's
+   solver; its MPC loop is Python around one solve per step,
+   python/bsqp/mpc_controller.py).  Fused-form solvers only; buffers in the
+   solver's scalar type.  For t = 0 .. steps-1: solve from x[t] with the goal
+   window d_goal_traj[b][6t, 6t+6N) ([B][6(N+steps)]), warm start d_xu
+   ([B][traj], its x_0 set to x[t]); apply u[t] = u_0 + noise[t]
+   (d_noise [steps][B][nu] or NULL) to the same dynamics for one dt into
+   x[t+1] (d_x [steps+1][B][nx], x[0] given); shift the warm start by one
+   knot.  d_ckpt_xu [steps][B][traj] and d_ckpt_rho [steps][B] (or NULL)
+   keep each step's solution and rho for gato_rollout_backward.  All steps
+   run as one CUDA graph (captured on the first call, replayed while the
+   pointers and step count stay the same). */
+int gato_rollout(gato_solver_t* s, void* stream, int steps, const void* d_goal_traj,
+                 void* d_xu, const void* d_noise, void* d_x, void* d_u,
+                 void* d_ckpt_xu, void* d_ckpt_rho);
+/* Reverse pass of a rollout for a loss of the states: from d_dl_dx
+   [steps+1][B][nx] gives dl/dx[0] [B][nx], dl/dgoal_traj [B][6(N+steps)] and
+   dl/d(Qd, Rd) [B][nx+nu] by chaining the simulator's step Jacobians with
+   gato_adjoint of every step (the controls' dependence on the state and on
+   the weights through each step's QP), from the checkpoints of
+   gato_rollout; dynamics derivatives are recomputed, the solver's rho is
+   restored afterwards.  tol / max_iters as in gato_adjoint.  Runs as one
+   CUDA graph and waits for it. */
+int gato_rollout_backward(gato_solver_t* s, void* stream, int steps,
+                          const void* d_goal_traj, const void* d_x, const void* d_u,
+                          const void* d_ckpt_xu, const void* d_ckpt_rho,
+                          const void* d_dl_dx, void* d_g_x0, void* d_g_goal_traj,
+                          void* d_g_wdiag, double tol, int max_iters);
+
 /* No counterpart in the reference.  The PCG of gato_stage_pcg (FP32 arithmetic
    and reductions, every problem solved) on caller-owned device buffers, with
    no solver handle and no device allocation, for callers that may not
