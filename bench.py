@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="problems in the CPU baseline sample (0: sized to ~10 s)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="single", choices=["single", "mixed"],
+    ap.add_argument("--workload", default="single", choices=["single", "mixed", "mpc"],
                     help="single: the headline iiwa14 N=32 batch; mixed: 4096 problems of "
                          "both plants and four horizons in one solve")
     return ap.parse_args()
@@ -739,8 +739,115 @@ def run_reference_mixed(args):
     return 0
 
 
+# --------------------------------------------------------------------------
+# closed-loop workload: per plant, N=128, batch 512, 50 receding-horizon steps
+# of 10 ms with seeded torque noise N(0, 0.05^2), figure-8 goals; forward
+# rollout (one graph) and its reverse pass into x0, goals and the Q/R
+# diagonals for a tracking loss; precision sweep against FP64
+MPC_N, MPC_B, MPC_STEPS = 128, 512, 50
+
+
+def run_mpc(args):
+    """Per plant and precision: forward rollout and reverse pass times (CUDA
+    events), the closed-loop state error against the FP64 rollout after 1, 10
+    and 50 steps, and the gradient error of the reverse pass run on the FP64
+    rollout's own trajectory and checkpoints (cast to the precision)."""
+    import ctypes
+    import torch
+    import gato_b200
+    import gato_b200._lib as L
+    from gato_b200 import mpc
+    from gato_b200 import workloads as W
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda")
+    steps = MPC_STEPS
+    # the reference's MPC settings (python/bsqp/config.py:36-51): one SQP
+    # iteration per control step (real-time iteration), PCG max 200 at 1e-4
+    kw = dict(max_sqp_iters=1, kkt_tol=1e-3, max_pcg_iters=200, pcg_tol=1e-4, solve_ratio=1.0,
+              mu=10.0, q_cost=2.0, qd_cost=1e-2, u_cost=2e-6, N_cost=50.0, q_lim_cost=0.01,
+              vel_lim_cost=0.0, ctrl_lim_cost=0.0, rho=0.01)
+    out = {"metric": "closed-loop MPC rollout (N=128, batch 512, 50 steps of 10 ms), ms",
+           "solver": "reference MPC settings, one SQP iteration per step",
+           "unit": "ms", "higher_is_better": False,
+           "loss": "sum over steps of |x_t - x_0|^2 (states of the closed loop)",
+           "plants": {}}
+
+    def backward(s, o, dt, gt):
+        B, nx = s.batch_size, s.nx
+        dl = (2 * (o["x"] - o["x"][0])).to(dt).contiguous()
+        dl[0] = 0
+        g_x0 = torch.empty((B, nx), dtype=dt, device=dev)
+        g_goal = torch.empty_like(gt)
+        g_w = torch.empty((B, nx + s.nu), dtype=dt, device=dev)
+        L.check(L.load().gato_rollout_backward(
+            s._h, None, steps, L.vptr(gt), L.vptr(o["x"]), L.vptr(o["u"]), L.vptr(o["ckpt_xu"]),
+            L.vptr(o["ckpt_rho"]), L.vptr(dl), L.vptr(g_x0), L.vptr(g_goal), L.vptr(g_w),
+            0.0, 0))
+        return g_w
+
+    for plant in ("indy7", "iiwa14"):
+        pr = W.make_problem(plant, MPC_N, MPC_B, seed=2028, goals="figure8", dt=DT)
+        rng = np.random.default_rng(2029)
+        nq = pr["model"].nq
+        gt_np = W.figure8_goals(pr["model"], pr["xs"], MPC_N + steps, DT, rng)
+        noise = rng.normal(0, 0.05, (steps, MPC_B, nq))
+        res, ref = {}, None
+        for prec in ("fp64", "mixed", "fp32"):
+            dt = torch.float64 if prec == "fp64" else torch.float32
+            T = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
+            s = gato_b200.BSQP(batch_size=MPC_B, N=MPC_N, dt=DT, plant_type=plant,
+                               precision=prec, **kw)
+            qd, rd = s.default_cost_diag()
+            s.set_cost_diag_batch(qd, rd)
+            x0, gt, nz = T(pr["xs"]), T(gt_np), T(noise)
+            fw, bw = [], []
+            for i in range(1 + max(1, args.steps // 25)):
+                s.reset_dual()
+                s.reset_rho()
+                torch.cuda.synchronize()
+                e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                e[0].record()
+                o = mpc.rollout(s, x0, gt, steps, nz)
+                e[1].record()
+                g_w = backward(s, o, dt, o["goal_traj"])
+                e[2].record()
+                torch.cuda.synchronize()
+                if i >= 1:
+                    fw.append(e[0].elapsed_time(e[1]))
+                    bw.append(e[1].elapsed_time(e[2]))
+            r = dict(forward_ms=float(np.mean(fw)), backward_ms=float(np.mean(bw)),
+                     x=o["x"].double().cpu().numpy(),
+                     nonfinite_x=int((~torch.isfinite(o["x"])).sum()),
+                     nonfinite_grad=int((~torch.isfinite(g_w)).sum()),
+                     max_abs_x=float(o["x"].abs().max()))
+            if prec == "fp64":
+                ref = dict(o=o, g_w=g_w.cpu().numpy(), gt=o["goal_traj"])
+            else:
+                # the reverse pass of this precision on the FP64 trajectory
+                o64 = {k: (v.to(dt) if torch.is_tensor(v) else v) for k, v in ref["o"].items()}
+                s.set_rho_penalty_batch(s.get_rho(), False)
+                gw = backward(s, o64, dt, o64["goal_traj"].contiguous()).double().cpu().numpy()
+                ok = np.isfinite(gw).all(axis=1) & np.isfinite(ref["g_w"]).all(axis=1)
+                r["grad_w_err_vs_fp64"] = float(np.abs(gw[ok] - ref["g_w"][ok]).max()
+                                                / np.abs(ref["g_w"][ok]).max())
+                r["grad_nonfinite_problems_on_fp64_traj"] = int((~ok).sum())
+            res[prec] = r
+            s.close()
+        x64 = res["fp64"]["x"]
+        scale = max(1.0, float(np.abs(x64).max()))
+        out["plants"][plant] = {
+            p: {k: v for k, v in r.items() if k != "x"} | {
+                f"x_err_vs_fp64_step{t}": float(np.abs(r["x"][t] - x64[t]).max() / scale)
+                for t in (1, 10, steps)}
+            for p, r in res.items()}
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "mpc":
+        return run_mpc(args)
     if args.workload == "mixed":
         return run_reference_mixed(args) if args.impl == "reference" else run_mixed(args)
     if args.impl == "reference":

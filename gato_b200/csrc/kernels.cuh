@@ -426,7 +426,7 @@ __device__ int pcg_block(int N, const T* __restrict__ S, const T* __restrict__ P
         part = btd_mv<NQ, T, Acc>(N, P, r, z, r);
         const Acc rho_new = block_sum<Acc>(part, red + WARP);
         const Acc arn = rho_new < 0 ? -rho_new : rho_new;
-        if (arn < abs_tol + (Acc)eps * rho_init) break;
+        if (arn < abs_tol + (Acc)eps * rho_init || !(arn > 0)) break;
         const Acc beta = rho_new / rho;
         rho = rho_new;
         const T bf = (T)beta;
@@ -679,12 +679,13 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
             if (!(fabs((double)rho) < (double)abs_tol)) {
                 const Acc rho_init = rho < 0 ? -rho : rho;
                 Acc alpha = rho / delta;
+                const bool start = isfinite((double)alpha);  // delta = 0: nothing to do
 #pragma unroll
                 for (int j = 0; j < RPT; ++j) {
                     p[j] = z[j];
                     sv[j] = w[j];
                 }
-                for (int it = 0; it < bt.max_pcg_iters; ++it) {
+                for (int it = 0; start && it < bt.max_pcg_iters; ++it) {
                     ++iters;
                     const T a = (T)alpha;
 #pragma unroll
@@ -710,9 +711,10 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
                     }
                     rows_block_sum2<Acc>(rho_new, delta, red);
                     const Acc arn = rho_new < 0 ? -rho_new : rho_new;
-                    if (arn < abs_tol + (Acc)eps * rho_init) break;
+                    if (arn < abs_tol + (Acc)eps * rho_init || !(arn > 0)) break;
                     const Acc beta = rho_new / rho;
                     alpha = rho_new / (delta - beta * rho_new / alpha);
+                    if (!isfinite((double)alpha)) break;  // breakdown: keep the iterate
                     rho = rho_new;
                     const T bb = (T)beta;
 #pragma unroll
@@ -747,6 +749,7 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
 #pragma unroll
                     for (int j = 0; j < RPT; ++j) part += act ? (Acc)p[j] * (Acc)ap[j] : Acc(0);
                     const Acc pap = rows_block_sum<Acc>(part, red);
+                    if (!(fabs((double)pap) > 0) || !isfinite((double)pap)) break;
                     const T alpha = (T)(rho / pap);
 #pragma unroll
                     for (int j = 0; j < RPT; ++j) {
@@ -761,7 +764,7 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
                     for (int j = 0; j < RPT; ++j) part += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);
                     const Acc rho_new = rows_block_sum<Acc>(part, red + WARP);
                     const Acc arn = rho_new < 0 ? -rho_new : rho_new;
-                    if (arn < abs_tol + (Acc)eps * rho_init) break;
+                    if (arn < abs_tol + (Acc)eps * rho_init || !(arn > 0)) break;
                     const T beta = (T)(rho_new / rho);
                     rho = rho_new;
 #pragma unroll

@@ -166,12 +166,13 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
             if (!(fabs((double)rho) < (double)abs_tol)) {
                 const Acc rho_init = rho < 0 ? -rho : rho;
                 Acc alpha = rho / delta;
+                const bool start = isfinite((double)alpha);  // delta = 0: nothing to do
 #pragma unroll
                 for (int j = 0; j < RPT; ++j) {
                     p[j] = z[j];
                     sv[j] = w[j];
                 }
-                for (int it = 0; it < bt.max_pcg_iters; ++it) {
+                for (int it = 0; start && it < bt.max_pcg_iters; ++it) {
                     ++iters;
                     const T a = (T)alpha;
 #pragma unroll
@@ -192,9 +193,10 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
                     }
                     csum2(rho_new, delta);
                     const Acc arn = rho_new < 0 ? -rho_new : rho_new;
-                    if (arn < abs_tol + (Acc)eps * rho_init) break;
+                    if (arn < abs_tol + (Acc)eps * rho_init || !(arn > 0)) break;
                     const Acc beta = rho_new / rho;
                     alpha = rho_new / (delta - beta * rho_new / alpha);
+                    if (!isfinite((double)alpha)) break;  // breakdown: keep the iterate
                     rho = rho_new;
                     const T bb = (T)beta;
 #pragma unroll
@@ -228,6 +230,7 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
 #pragma unroll
                     for (int j = 0; j < RPT; ++j) pap += act ? (Acc)p[j] * (Acc)w[j] : Acc(0);
                     csum2(pap, unused);
+                    if (!(fabs((double)pap) > 0) || !isfinite((double)pap)) break;
                     const T alpha = (T)(rho / pap);
 #pragma unroll
                     for (int j = 0; j < RPT; ++j) {
@@ -242,7 +245,7 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
                     for (int j = 0; j < RPT; ++j) rho_new += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);
                     csum2(rho_new, unused);
                     const Acc arn = rho_new < 0 ? -rho_new : rho_new;
-                    if (arn < abs_tol + (Acc)eps * rho_init) break;
+                    if (arn < abs_tol + (Acc)eps * rho_init || !(arn > 0)) break;
                     const T beta = (T)(rho_new / rho);
                     rho = rho_new;
 #pragma unroll
