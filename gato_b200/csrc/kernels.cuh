@@ -236,7 +236,7 @@ __device__ __forceinline__ void merit_ls_body(const Batch<NQ, T>& bt, const DevM
 }
 
 template <int NQ, typename T, typename Acc>
-__global__ void __launch_bounds__(256) k_merit_ls(Batch<NQ, T> bt, DevModel<NQ, T> M, int mode,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_merit_ls(Batch<NQ, T> bt, DevModel<NQ, T> M, int mode,
                                                   int it)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1077,7 +1077,7 @@ __device__ __forceinline__ void fused_iter_body(const Batch<NQ, T>& bt, const De
 }
 
 template <int NQ, typename T, typename Acc>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1)
     k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int it_row, int with_pcg)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
