@@ -47,7 +47,7 @@ __device__ __forceinline__ int queue_next(int* head, int nitems, int* s_item)
 // warps split into PPB teams that pull work independently, each with
 // team_bytes of shared memory).
 template <typename T, typename Acc, int KG, int PPB>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     k_q_fused_iter(MultiArgs<T> ma, int it_row, int team_bytes)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
