@@ -716,7 +716,7 @@ def run_mixed(args):
         "data": "synthetic (seeded draw of plants/horizons, figure-8 goals, rho ~ logU[1e-2,1e2])",
         "config": {"workload": "mixed 4096", "classes": classes, "sqp_iters": SQP_ITERS,
                    "l2": "flushed between steps"},
-        "tuner_ms": {f"lanes{k[0]}_ppb{k[1]}": v for k, v in shapes.items()},
+        "tuner_ms": {f"lanes{k[0]}_ppb{k[1]}_ctas{k[2]}": v for k, v in shapes.items()},
         "per_class": [{"plant": p, "N": n, "count": c, "alone_ms": a,
                        "pcg_iters_mean": float(np.mean(st["pcg_iters"]))}
                       for (p, n, c), a, st in zip(classes, alone, stats)],

@@ -129,7 +129,7 @@ SIGNATURES = {
                                         ctypes.POINTER(_vp)]),
     "gato_mixed_stats": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(GatoStats)]),
     "gato_mixed_elapsed_ms": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
-    "gato_mixed_config": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "gato_mixed_config": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "gato_mixed_tune": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
                                        ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_float)]),
     "gato_adjoint": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,

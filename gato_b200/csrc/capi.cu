@@ -1785,7 +1785,7 @@ struct gato_mixed {
     cudaGraphExec_t gexec = nullptr;
     std::vector<const void*> gkey;
     long gver = -1;
-    int kg = 16, ppb = 1;  // KKT lanes per knot, problems per CTA (gato_mixed_tune)
+    int kg = 16, ppb = 1, occ = 2;  // KKT lanes per knot, problems per CTA, CTAs per SM
 };
 
 namespace {
@@ -1815,7 +1815,7 @@ bool rows_fit(const gato_solver* s)
     return s->nq == 7 ? RowPcg<7, RPT>::fits(s->N) : RowPcg<6, RPT>::fits(s->N);
 }
 
-template <typename T, typename Acc, int KG, int PPB>
+template <typename T, typename Acc, int KG, int PPB, int MINB>
 int launch_q_fused(gato_mixed* mx, cudaStream_t st, const MultiArgs<T>& ma, int it)
 {
     int team_bytes = 0;
@@ -1827,7 +1827,7 @@ int launch_q_fused(gato_mixed* mx, cudaStream_t st, const MultiArgs<T>& ma, int 
         team_bytes = std::max(team_bytes, (int)((by + 255) & ~(size_t)255));
     }
     const size_t smem = (size_t)PPB * team_bytes;
-    auto kern = k_q_fused_iter<T, Acc, KG, PPB>;
+    auto kern = k_q_fused_iter<T, Acc, KG, PPB, MINB>;
     if (smem > 48 * 1024)
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
@@ -1841,11 +1841,17 @@ int launch_q_fused(gato_mixed* mx, cudaStream_t st, const MultiArgs<T>& ma, int 
 template <typename T, typename Acc>
 int launch_q_fused_any(gato_mixed* mx, cudaStream_t st, const MultiArgs<T>& ma, int it)
 {
-    if (mx->kg == 32)
-        return mx->ppb == 2 ? launch_q_fused<T, Acc, 32, 2>(mx, st, ma, it)
-                            : launch_q_fused<T, Acc, 32, 1>(mx, st, ma, it);
-    return mx->ppb == 2 ? launch_q_fused<T, Acc, 16, 2>(mx, st, ma, it)
-                        : launch_q_fused<T, Acc, 16, 1>(mx, st, ma, it);
+    const int sel = (mx->kg == 32 ? 4 : 0) + (mx->ppb == 2 ? 2 : 0) + (mx->occ == 4 ? 1 : 0);
+    switch (sel) {
+        case 0: return launch_q_fused<T, Acc, 16, 1, 2>(mx, st, ma, it);
+        case 1: return launch_q_fused<T, Acc, 16, 1, 4>(mx, st, ma, it);
+        case 2: return launch_q_fused<T, Acc, 16, 2, 2>(mx, st, ma, it);
+        case 3: return launch_q_fused<T, Acc, 16, 2, 4>(mx, st, ma, it);
+        case 4: return launch_q_fused<T, Acc, 32, 1, 2>(mx, st, ma, it);
+        case 5: return launch_q_fused<T, Acc, 32, 1, 4>(mx, st, ma, it);
+        case 6: return launch_q_fused<T, Acc, 32, 2, 2>(mx, st, ma, it);
+        default: return launch_q_fused<T, Acc, 32, 2, 4>(mx, st, ma, it);
+    }
 }
 
 template <typename T, typename Acc>
@@ -1948,7 +1954,7 @@ int mixed_enqueue(gato_mixed* mx, cudaStream_t st, void* const* xu, const void* 
 
 long mixed_version(const gato_mixed* mx)
 {
-    long v = mx->kg * 7 + mx->ppb;
+    long v = (mx->kg * 7 + mx->ppb) * 5 + mx->occ;
     for (int c = 0; c < mx->ncls; ++c) v = v * 131 + mx->cls[c]->version;
     return v;
 }
@@ -2142,14 +2148,17 @@ int gato_mixed_elapsed_ms(gato_mixed_t* mx, float* ms)
     return GATO_OK;
 }
 
-int gato_mixed_config(gato_mixed_t* mx, int lanes_per_knot, int problems_per_block)
+int gato_mixed_config(gato_mixed_t* mx, int lanes_per_knot, int problems_per_block,
+                      int ctas_per_sm)
 {
     RC(check_mixed(mx));
     if ((lanes_per_knot != 16 && lanes_per_knot != 32) ||
-        (problems_per_block != 1 && problems_per_block != 2))
-        return fail(GATO_ERR_ARG, "lanes per knot 16|32, problems per block 1|2");
+        (problems_per_block != 1 && problems_per_block != 2) ||
+        (ctas_per_sm != 2 && ctas_per_sm != 4))
+        return fail(GATO_ERR_ARG, "lanes per knot 16|32, problems per block 1|2, CTAs per SM 2|4");
     mx->kg = lanes_per_knot;
     mx->ppb = problems_per_block;
+    mx->occ = ctas_per_sm;
     return GATO_OK;
 }
 
@@ -2158,7 +2167,8 @@ int gato_mixed_tune(gato_mixed_t* mx, void* stream, void* const* d_xu, const voi
 {
     RC(check_mixed(mx));
     cudaStream_t st = as_stream(stream);
-    const int cand[4][2] = {{16, 1}, {16, 2}, {32, 1}, {32, 2}};
+    const int cand[8][3] = {{16, 1, 2}, {16, 1, 4}, {16, 2, 2}, {16, 2, 4},
+                            {32, 1, 2}, {32, 1, 4}, {32, 2, 2}, {32, 2, 4}};
     // the solve changes XU, lambda, rho and drho: keep copies, restore them
     // before every trial and at the end
     std::vector<void*> saved;
@@ -2201,9 +2211,10 @@ int gato_mixed_tune(gato_mixed_t* mx, void* stream, void* const* d_xu, const voi
     };
     int best = 0, rc = GATO_OK;
     float best_ms = 1e30f;
-    for (int i = 0; i < 4 && rc == GATO_OK; ++i) {
+    for (int i = 0; i < 8 && rc == GATO_OK; ++i) {
         mx->kg = cand[i][0];
         mx->ppb = cand[i][1];
+        mx->occ = cand[i][2];
         float t = 0.0f;
         for (int rep = 0; rep < 2 && rc == GATO_OK; ++rep) {  // the first run warms up
             restore();
@@ -2221,6 +2232,7 @@ int gato_mixed_tune(gato_mixed_t* mx, void* stream, void* const* d_xu, const voi
     for (void* p : saved) cudaFree(p);
     mx->kg = cand[best][0];
     mx->ppb = cand[best][1];
+    mx->occ = cand[best][2];
     return rc;
 }
 

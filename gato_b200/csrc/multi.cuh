@@ -45,9 +45,10 @@ __device__ __forceinline__ int queue_next(int* head, int nitems, int* s_item)
 // KKT + Schur system of every queued problem (S, P^-1, gamma to global
 // memory).  KG lanes per knot; PPB problems per CTA at a time (the CTA's
 // warps split into PPB teams that pull work independently, each with
-// team_bytes of shared memory).
-template <typename T, typename Acc, int KG, int PPB>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+// team_bytes of shared memory); MINB CTAs per SM in FP32 (registers traded
+// for resident warps).
+template <typename T, typename Acc, int KG, int PPB, int MINB>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? MINB : 1)
     k_q_fused_iter(MultiArgs<T> ma, int it_row, int team_bytes)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -25,7 +25,9 @@ PARAM_KEYS = ("max_sqp_iters", "kkt_tol", "max_pcg_iters", "pcg_tol", "solve_rat
 DEFAULTS = dict(max_sqp_iters=10, kkt_tol=1e-4, max_pcg_iters=100, pcg_tol=1e-4,
                 solve_ratio=1.0, mu=1.0, q_cost=2.0, qd_cost=1e-4, u_cost=1e-6, N_cost=50.0,
                 q_lim_cost=1e-3, vel_lim_cost=0.0, ctrl_lim_cost=0.0, rho=0.0)
-SHAPES = ((16, 1), (16, 2), (32, 1), (32, 2))  # (lanes per knot, problems per CTA)
+# (lanes per knot, problems per CTA, CTAs per SM)
+SHAPES = ((16, 1, 2), (16, 1, 4), (16, 2, 2), (16, 2, 4), (32, 1, 2), (32, 1, 4), (32, 2, 2),
+          (32, 2, 4))
 
 
 class MixedBSQP:
@@ -89,8 +91,9 @@ class MixedBSQP:
                 "final_merit": bufs["final_merit"], "initial_merit": bufs["initial_merit"],
                 "ls_step_size": bufs["ls_step_size"][: n * B].reshape(n, B)}
 
-    def config(self, lanes_per_knot=16, problems_per_block=1):
-        L.check(L.load().gato_mixed_config(self._h, int(lanes_per_knot), int(problems_per_block)))
+    def config(self, lanes_per_knot=16, problems_per_block=1, ctas_per_sm=2):
+        L.check(L.load().gato_mixed_config(self._h, int(lanes_per_knot), int(problems_per_block),
+                                           int(ctas_per_sm)))
 
     def tune(self, xu, xs, goal, stream=0):
         """Autotuner: times each launch shape on these inputs (state restored
@@ -98,6 +101,6 @@ class MixedBSQP:
         pa, ka = self._ptrs(xu)
         pb, kb = self._ptrs(xs)
         pc, kc = self._ptrs(goal)
-        ms = (ctypes.c_float * 4)()
+        ms = (ctypes.c_float * len(SHAPES))()
         L.check(L.load().gato_mixed_tune(self._h, ctypes.c_void_p(int(stream)), pa, pb, pc, ms))
-        return {SHAPES[i]: float(ms[i]) for i in range(4)}
+        return {SHAPES[i]: float(ms[i]) for i in range(len(SHAPES))}

@@ -382,14 +382,16 @@ int gato_mixed_solve(gato_mixed_t* mx, void* stream, void* const* d_xu,
 int gato_mixed_stats(gato_mixed_t* mx, int c, gato_stats_t* stats);
 /* device time of the last solve in ms (waits for it) */
 int gato_mixed_elapsed_ms(gato_mixed_t* mx, float* ms);
-/* KKT-stage launch shape: lanes per knot (16: two knots per warp, 32: one)
-   and problems per CTA (1 or 2) */
+/* KKT-stage launch shape: lanes per knot (16: two knots per warp, 32: one),
+   problems per CTA (1 or 2) and CTAs per SM (2 or 4: registers per thread
+   traded for resident warps) */
 int gato_mixed_config(gato_mixed_t* mx, int lanes_per_knot,
-                      int problems_per_block);
+                      int problems_per_block, int ctas_per_sm);
 /* Autotuner: times the solve of these inputs under each launch shape
-   (lanes per knot x problems per CTA, in the order (16,1) (16,2) (32,1)
-   (32,2), ms_out[4] optional), restores XU, lambda, rho and drho after every
-   trial, and keeps the fastest shape.  Allocates temporary copies. */
+   (lanes per knot x problems per CTA x CTAs per SM, in the order (16,1,2)
+   (16,1,4) (16,2,2) (16,2,4) (32,1,2) (32,1,4) (32,2,2) (32,2,4); ms_out[8]
+   optional), restores XU, lambda, rho and drho after every trial, and keeps
+   the fastest shape.  Allocates temporary copies. */
 int gato_mixed_tune(gato_mixed_t* mx, void* stream, void* const* d_xu,
                     const void* const* d_xs, const void* const* d_goal,
                     float* ms_out);

@@ -40,12 +40,13 @@ def test_mixed_solve_matches_classes_solved_alone(precision):
     dt = torch.float64 if precision == "fp64" else torch.float32
     data, T = _inputs(torch, dt, 50)
     mx = MixedBSQP(CLASSES, precision=precision, **PARAMS_CFG2)
-    shapes = [(16, 1)] if precision == "fp64" else [(16, 1), (16, 2), (32, 1), (32, 2)]
-    for kg, ppb in shapes:
+    from gato_b200.mixed import SHAPES
+    shapes = [(16, 1, 2)] if precision == "fp64" else list(SHAPES)
+    for kg, ppb, occ in shapes:
         for c in mx.cls:
             c.reset_dual()
             c.reset_rho()
-        mx.config(kg, ppb)
+        mx.config(kg, ppb, occ)
         xu = [T(pr["xu"]) for pr in data]
         mx.solve_device(xu, [T(pr["xs"]) for pr in data], [T(pr["goal"]) for pr in data])
         torch.cuda.synchronize()
