@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="problems in the CPU baseline sample (0: sized to ~10 s)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="single", choices=["single", "mixed", "mpc"],
+    ap.add_argument("--workload", default="single", choices=["single", "mixed", "mpc", "sweep"],
                     help="single: the headline iiwa14 N=32 batch; mixed: 4096 problems of "
                          "both plants and four horizons in one solve")
     return ap.parse_args()
@@ -223,18 +223,22 @@ def fp32_peak_tflops(torch, dev):
 
 
 # --------------------------------------------------------------------------
-def cpu_baseline(wl, sample, threads):
+def cpu_baseline(wl, sample, threads, with_result=False):
     """The FP64 oracle of the same SQP on `sample` problems of the workload,
-    `threads` host threads; returns (solves/s, seconds)."""
+    `threads` host threads; returns (solves/s, seconds) and, with_result,
+    the oracle's trajectories and statistics (the checker of the GPU
+    solution of the same problems)."""
     from oracle import oracle as O
     kw = solver_kwargs()
     P = O.make_params(dt=DT, **kw)
     S = O.Solver(PLANT, N, sample, P, threads=threads)
     S.set_lambda(wl["lam"][:sample].astype(np.float64))
     t0 = time.perf_counter()
-    S.solve(wl["xu"][:sample].astype(np.float64), DT, wl["xs"][:sample].astype(np.float64),
-            wl["goal"][:sample].astype(np.float64))
+    xo, so = S.solve(wl["xu"][:sample].astype(np.float64), DT,
+                     wl["xs"][:sample].astype(np.float64), wl["goal"][:sample].astype(np.float64))
     dt = time.perf_counter() - t0
+    if with_result:
+        return sample / dt, dt, xo, so
     return sample / dt, dt
 
 
@@ -272,7 +276,10 @@ def run_reference(args):
     return 0
 
 
-def reference_gpu_leg(args):
+_REF_MODULE = {}
+
+
+def reference_gpu_leg(args, B=None):
     """The reference's own CUDA solver (python/bindings.cu compiled unmodified
     for sm_100a into oracle/_ref by oracle/build_ref_gpu.py) on the same
     workload, through its own solve(): host arrays in, host arrays out, as
@@ -291,10 +298,13 @@ def reference_gpu_leg(args):
     except ImportError:
         return {"unavailable": "torch missing"}
     name = f"bsqpN{N}_{PLANT}"
-    spec = importlib.util.spec_from_file_location(name, paths[0])
-    mod = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(mod)
-    B = args.batch
+    if name not in _REF_MODULE:  # a pybind11 module loads once per process
+        spec = importlib.util.spec_from_file_location(name, paths[0])
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        _REF_MODULE[name] = mod
+    mod = _REF_MODULE[name]
+    B = B or args.batch
     cls = getattr(mod, f"BSQP_{B}_float", None)
     if cls is None:
         return {"unavailable": f"the reference module has no batch-{B} class"}
@@ -335,6 +345,7 @@ def reference_gpu_leg(args):
     return {"value": B / float(np.mean(wall)), "unit": "solves/s",
             "own_timer_value": B / float(np.mean(own)),
             "ms_per_step": 1e3 * float(np.mean(wall)),
+            "p50_ms": 1e3 * float(np.median(wall)), "p99_ms": 1e3 * float(np.percentile(wall, 99)),
             "kind": "reference CUDA build, FP32 -use_fast_math, sm_100a",
             "note": "solve() with host arrays (its own H2D/D2H inside); lambda carried "
                     "between calls as the reference keeps it; rho reset before each call",
@@ -532,10 +543,25 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         sample = args.cpu_sample or int(min(B, max(threads, 64 * threads)))
-        v, secs = cpu_baseline(wl, sample, threads)
+        v, secs, xo, so = cpu_baseline(wl, sample, threads, with_result=True)
         cpu = {"value": v, "unit": "solves/s", "cores": threads, "kind": "port",
                "sample": f"{sample} problems of the workload, one solve, {secs:.1f} s wall "
                          f"(FP64 oracle port of the reference SQP)"}
+        # the oracle as the checker: the FP32 solution of the same problems
+        # from the same warm start, lambda and rho
+        d_xu.copy_(d_xu0)
+        fused.set_lambda(wl["lam"])
+        fused.reset_rho()
+        stg = fused.solve_device(d_xu, d_xs, d_goal, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        xg = d_xu.double().cpu().numpy()[:sample]
+        errs = np.abs(xg - xo).max(axis=1) / np.maximum(1.0, np.abs(xo).max(axis=1))
+        accuracy = {"sample": sample, "xu_rel_err_max": float(errs.max()),
+                    "xu_rel_err_median": float(np.median(errs)),
+                    "pcg_iters_equal_frac": float(np.mean(
+                        stg["pcg_iters"][:, :sample] == so["pcg_iters"]))
+                    if stg["pcg_iters"].shape[0] == so["pcg_iters"].shape[0] else None,
+                    "note": "FP32 fused solve vs the FP64 oracle of the same SQP, same inputs"}
     if dist:
         dist.destroy_process_group()
     if rank != 0:
@@ -598,6 +624,7 @@ def run_ours(args):
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+        line["accuracy_vs_fp64_oracle"] = accuracy
     print(json.dumps(line))
     return 0
 
@@ -844,8 +871,67 @@ def run_mpc(args):
     return 0
 
 
+# --------------------------------------------------------------------------
+# batch-size sweep of the headline workload (iiwa14 N=32, 5 SQP iterations)
+SWEEP_BATCHES = (1, 32, 128, 512, 1024)
+
+
+def run_sweep(args):
+    import torch
+    import gato_b200
+    import gato_b200._lib as L
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda")
+    kw = solver_kwargs()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    rows = []
+    for B in SWEEP_BATCHES:
+        wl = make_workload(B, seed=2026)
+        s = gato_b200.BSQP(batch_size=B, N=N, dt=DT, plant_type=PLANT, form="fused", **kw)
+        T = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
+        d_xu0, d_xs, d_goal = T(wl["xu"]), T(wl["xs"]), T(wl["goal"])
+        d_xu = d_xu0.clone()
+        t = time_device_steps(torch, s, (d_xu, d_xs, d_goal, d_xu0), wl, args.steps,
+                              args.warmup, flush, stream)
+        h_xu = torch.empty(tuple(d_xu.shape), dtype=torch.float32).pin_memory()
+        h_xs, h_goal = torch.tensor(wl["xs"]).pin_memory(), torch.tensor(wl["goal"]).pin_memory()
+        e2e = []
+        for i in range(args.warmup + args.steps):
+            h_xu.copy_(torch.from_numpy(wl["xu"]))
+            s.set_lambda(wl["lam"])
+            s.reset_rho()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            L.check(L.load().gato_solve_host(s._h, L.fptr(h_xu), DT, L.fptr(h_xs),
+                                             L.fptr(h_goal), None))
+            if i >= args.warmup:
+                e2e.append(1e3 * (time.perf_counter() - t0))
+        s.close()
+        rows.append({"batch": B, "solves_per_s": B / (float(np.mean(t)) * 1e-3),
+                     "p50_ms": float(np.median(t)), "p99_ms": float(np.percentile(t, 99)),
+                     "e2e_solves_per_s": B / (float(np.mean(e2e)) * 1e-3),
+                     "e2e_p50_ms": float(np.median(e2e)), "e2e_p99_ms": float(np.percentile(e2e, 99))})
+    print(json.dumps({"metric": "SQP solves/s and latency vs batch size (iiwa14 N=32, 5 SQP iters)",
+                      "unit": "solves/s", "rows": rows}))
+    return 0
+
+
+def run_reference_sweep(args):
+    rows = []
+    for B in SWEEP_BATCHES:
+        r = reference_gpu_leg(args, B)
+        r["batch"] = B
+        rows.append(r)
+    print(json.dumps({"impl": "reference", "metric": "SQP solves/s and latency vs batch size "
+                      "(iiwa14 N=32, 5 SQP iters)", "unit": "solves/s", "rows": rows}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "sweep":
+        return run_reference_sweep(args) if args.impl == "reference" else run_sweep(args)
     if args.workload == "mpc":
         return run_mpc(args)
     if args.workload == "mixed":
