@@ -50,6 +50,7 @@ int gato_create(const gato_model_t* model, int N, int batch, const gato_params_t
     p->dt = params->dt;
     CK(cudaGetDevice(&p->device));
     CK(cudaDeviceGetAttribute(&p->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device));
+    CK(cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, p->device));
     dispatch(p, [&](auto tg) {
         using Tg = decltype(tg);
         build_dev_model<Tg::NQ, typename Tg::T>(*model,

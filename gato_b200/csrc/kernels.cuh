@@ -253,7 +253,7 @@ __global__ void k_kkt(Batch<NQ, T> bt, DevModel<NQ, T> M)
     const int wpb = blockDim.x / WARP;
     const int k = blockIdx.x * wpb + warp_id();
     const int N = bt.N;
-    if (k >= N - 1) return;
+    if (k >= N - 1 || *bt.done) return;  // done: a converged fused-form batch
     const Dims<NQ> d{N};
     constexpr int nx = Dims<NQ>::nx, nu = Dims<NQ>::nu;
     T* s = smem + warp_id() * KktSmem<NQ>::SIZE;
@@ -983,7 +983,8 @@ template <int NQ, typename T, typename Acc, int KG = 16>
 __device__ __forceinline__ void fused_iter_body(const Batch<NQ, T>& bt, const DevModel<NQ, T>& M,
                                                 int b, int stage, int it_row, int with_pcg,
                                                 unsigned char* smem_raw,
-                                                const Team& team = Team::cta())
+                                                const Team& team = Team::cta(),
+                                                bool with_kkt = true)
 {
     T* smem = reinterpret_cast<T*>(smem_raw);
     if (*bt.done) return;
@@ -1016,8 +1017,10 @@ __device__ __forceinline__ void fused_iter_body(const Batch<NQ, T>& bt, const De
     const T* xu = bt.xu + (size_t)b * d.traj();
     const T* fext = bt.use_fext ? bt.fext + 6 * b : nullptr;
 
-    // KKT set-up, two knots per warp (one per half-warp) or one per warp
-    if constexpr (KG == 32) {
+    // KKT set-up, two knots per warp (one per half-warp) or one per warp;
+    // skipped when a knot-parallel KKT kernel already wrote the blocks
+    if (!with_kkt) {
+    } else if constexpr (KG == 32) {
         for (int k = wid; k < N - 1; k += nw)
             kkt_knot<NQ, T, 32>(M, cost_of<NQ>(bt.cp, b), N, k, xu, bt.xs + (size_t)b * nx,
                                 bt.goal + (size_t)b * d.goal(), fext, Q, R, qv, rv, A, Bm, c,
@@ -1078,10 +1081,12 @@ __device__ __forceinline__ void fused_iter_body(const Batch<NQ, T>& bt, const De
 
 template <int NQ, typename T, typename Acc>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1)
-    k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int it_row, int with_pcg)
+    k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int it_row, int with_pcg,
+                 int with_kkt)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    fused_iter_body<NQ, T, Acc>(bt, M, blockIdx.x, stage, it_row, with_pcg, smem_raw);
+    fused_iter_body<NQ, T, Acc>(bt, M, blockIdx.x, stage, it_row, with_pcg, smem_raw,
+                                Team::cta(), with_kkt != 0);
 }
 
 }  // namespace gato

@@ -178,6 +178,7 @@ struct gato_solver {
     void* wdiag = nullptr;  // [B][nx+nu] diagonal cost weights, allocated on first use
     int use_wdiag = 0;
     int max_smem = 0;
+    int nsm = 148;  // SMs of the device
     // device memory, scalar-typed buffers as raw pointers
     void *xu = nullptr, *xs = nullptr, *goal = nullptr, *fext = nullptr;
     void *Q = nullptr, *R = nullptr, *q = nullptr, *r = nullptr, *A = nullptr, *Bm = nullptr,
@@ -497,13 +498,20 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
     // rows of S and P^-1 per thread in k_pcg_rows: two in FP32 (each window
     // value loaded from shared memory feeds two rows), one in FP64 (registers)
     constexpr int RPT = sizeof(T) == 4 ? 2 : 1;
+    // Fewer problems than half the SMs: one CTA per problem would leave SMs
+    // idle and make every problem's KKT blocks a serial chain of knots, so
+    // the KKT runs knot-parallel (k_kkt, a warp per knot) and the fused
+    // kernel starts at the Schur complement (measured: B = 1 and 32 gain
+    // 15-18 %, B = 128 loses 5 %).
+    const int with_kkt = 2 * s->B > s->nsm;
+    if (!with_kkt) RC(launch_kkt<Tg>(s, st, bt));
     if (RowPcg<NQ, RPT>::fits(s->N)) {
         // KKT + Schur into global memory, then the register-resident PCG + dz
         {
             ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
             FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, false};
-            k_fused_iter<NQ, T, Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(bt, dmodel<Tg>(s),
-                                                                              0, row, 0);
+            k_fused_iter<NQ, T, Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(
+                bt, dmodel<Tg>(s), 0, row, 0, with_kkt);
             CKL();
         }
         ProfScope ps2_(s, st, GATO_KERNEL_PCG);
@@ -517,8 +525,8 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
         {
             ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
             FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, false};
-            k_fused_iter<NQ, T, Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(bt, dmodel<Tg>(s),
-                                                                              0, row, 0);
+            k_fused_iter<NQ, T, Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(
+                bt, dmodel<Tg>(s), 0, row, 0, with_kkt);
             CKL();
         }
         return launch_pcg_cluster<Tg>(s, st, bt, row);
@@ -527,7 +535,7 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
     const bool stage = fused_stage_fits<Tg>(s);
     FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, stage};
     k_fused_iter<NQ, T, Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(bt, dmodel<Tg>(s), stage,
-                                                                      row, 1);
+                                                                      row, 1, with_kkt);
     CKL();
     return GATO_OK;
 }
