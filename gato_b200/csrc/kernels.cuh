@@ -271,8 +271,6 @@ __global__ void k_kkt(Batch<NQ, T> bt, DevModel<NQ, T> M)
 template <int NQ, typename T>
 __global__ void k_schur_inv(Batch<NQ, T> bt)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* smem = reinterpret_cast<T*>(smem_raw);
     const int b = blockIdx.y;
     const int wpb = blockDim.x / WARP;
     const int k = blockIdx.x * wpb + warp_id();
@@ -282,7 +280,7 @@ __global__ void k_schur_inv(Batch<NQ, T> bt)
     const T rho = bt.rho[b];
     const T* Qk = bt.Q + ((size_t)b * N + k) * nx * nx;
     warp_invert<nx, T>(Qk, rho, bt.Qi + ((size_t)b * N + k) * nx * nx);
-    if (k < N - 1) warp_invert<nu, T>(bt.R + ((size_t)b * N + k) * nu * nu, 0.0f,
+    if (k < N - 1) warp_invert<nu, T>(bt.R + ((size_t)b * N + k) * nu * nu, T(0),
                                    bt.Ri + ((size_t)b * N + k) * nu * nu);
 }
 

@@ -97,9 +97,7 @@ int enqueue_mixed(gato_mixed* mx, cudaStream_t st, void* const* xu, const void* 
     bool has_long = false;
     for (int c = 0; c < mx->ncls; ++c) {
         gato_solver* s = mx->cls[c];
-        const Dims<7> d7{s->N};
         const size_t traj = (size_t)(3 * s->nq) * s->N - s->nq;
-        (void)d7;
         CK(cudaMemsetAsync(s->dz, 0, s->esz * (size_t)s->B * traj, st));
         CK(cudaMemsetAsync(s->conv, 0, sizeof(int) * s->B, st));
         CK(cudaMemsetAsync(s->sqp_iters, 0, sizeof(int) * s->B, st));
