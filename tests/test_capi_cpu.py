@@ -54,6 +54,31 @@ def test_argument_errors_need_no_gpu():
             gato_b200.BSQP(**args)
 
 
+def test_extension_entry_points_validate_before_touching_the_gpu():
+    """Argument errors of the entry points without a reference counterpart
+    come back as GATO_ERR_ARG with a message, before any CUDA call."""
+    import ctypes
+    import gato_b200._lib as L
+    lib = L.load()
+    h = ctypes.c_void_p()
+    P = L.GatoParams(dt=0.01, max_sqp_iters=1, max_pcg_iters=10, pcg_tol=1e-5, solve_ratio=1.0)
+    assert lib.gato_mixed_create(None, 0, ctypes.byref(P), 0, ctypes.byref(h)) == -1
+    cls = (L.GatoClass * 9)(*[L.GatoClass(0, 8, 1) for _ in range(9)])
+    assert lib.gato_mixed_create(cls, 9, ctypes.byref(P), 0, ctypes.byref(h)) == -1
+    assert b"classes" in lib.gato_last_error()
+    assert lib.gato_mixed_solve(None, None, None, None, None) == -1
+    assert lib.gato_adjoint(None, None, None, None, None, None, None, None, None, 0.0, 0,
+                            None) == -1
+    assert lib.gato_rollout(None, None, 1, None, None, None, None, None, None, None) == -1
+    assert lib.gato_rollout_backward(None, None, 1, None, None, None, None, None, None, None,
+                                     None, None, 0.0, 0) == -1
+    assert lib.gato_set_cost_diag_batch(None, None) == -1
+    buf = ctypes.c_void_p(16)
+    assert lib.gato_pcg_static(None, 7, 32, 0, 1e-5, 10, buf, buf, buf, buf, buf) == -1
+    assert lib.gato_pcg_static(None, 5, 32, 4, 1e-5, 10, buf, buf, buf, buf, buf) == -3
+    assert lib.gato_pcg_static(None, 7, 32, 4, 1e-5, 10, None, buf, buf, buf, buf) == -1
+
+
 def test_unsupported_joint_count():
     import gato_b200
     import gato_b200._lib as L
