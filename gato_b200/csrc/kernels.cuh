@@ -492,13 +492,32 @@ __global__ void k_pcg(Batch<NQ, T> bt, int stage, int it_row)
 // RPT rows of one block row of S and P^-1 (3n entries per row) and the
 // matching entries of every CG vector; only p and r go through shared memory,
 // where a thread reads the 3n-wide window of its block row once with 16-byte
-// loads and applies it to all of its rows.  Vectors use a block stride VS (n
-// rounded up to a multiple of 4) so windows are aligned.  Same iteration as
-// pcg_block (gato/bsqp/kernels/pcg.cuh:23-147).  After the solve the block
-// computes the step dz of every knot (dz_knot's algebra).
+// loads and applies it to all of its rows.  Same iteration as pcg_block
+// (gato/bsqp/kernels/pcg.cuh:23-147).  After the solve the block computes the
+// step dz of every knot (dz_knot's algebra).
+//
+// Vectors use a block stride VS: n rounded up to a multiple of 4 whose number
+// of 16-byte chunks is odd.  A warp reads the windows of five or six
+// consecutive block rows at once; with an odd chunk count those start in
+// different bank quads (iiwa14: VS = 20, not 16, which put every other block
+// row on the same banks and serialised the load three ways).
+__host__ __device__ constexpr int row_vs(int n)
+{
+    return (((n + 3) / 4) % 2) ? ((n + 3) & ~3) : ((n + 3) & ~3) + 4;
+}
+
+// Rows of S and P^-1 per thread in the register-resident PCG: two in FP32
+// (each window value loaded from shared memory feeds two rows; one row per
+// thread measured 13 % slower), one in FP64.
+template <typename T>
+__host__ __device__ constexpr int pcg_rows_per_thread()
+{
+    return sizeof(T) == 4 ? 2 : 1;
+}
+
 template <int NQ, int RPT>
 struct RowPcg {
-    static constexpr int n = 2 * NQ, m = NQ, RD = 3 * n, VS = (n + 3) & ~3;
+    static constexpr int n = 2 * NQ, m = NQ, RD = 3 * n, VS = row_vs(n);
     static constexpr int TPB = n / RPT;  // threads per block row
     static_assert(n % RPT == 0, "rows per thread must divide n");
     static constexpr int MAX_THREADS = 512 / RPT;
@@ -511,34 +530,46 @@ struct RowPcg {
     }
 };
 
-template <typename T>
-struct Vec16;
-template <>
-struct Vec16<float> {
-    static constexpr int W = 4;
-    __device__ static void load(const float* p, float* o)
+// The RPT rows of S or P^-1 a thread holds in registers.  FP32 rows are kept
+// as column pairs, so one packed FMA (__ffma2_rn: each lane rounded as
+// fmaf) advances the even- and odd-column partial sums of a row together.
+template <int NQ, int RPT, typename T>
+struct RowMat {
+    static constexpr int RD = 6 * NQ;
+    T v[RPT][RD];
+    // rows j = 0..RPT-1 start at base + j * jstride (zero rows when !act)
+    __device__ __forceinline__ void load(const T* base, size_t jstride, bool act)
     {
-        const float4 v = *reinterpret_cast<const float4*>(p);
-        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+#pragma unroll
+        for (int j = 0; j < RPT; ++j)
+#pragma unroll
+            for (int c = 0; c < RD; ++c) v[j][c] = act ? base[j * jstride + c] : T(0);
     }
 };
-template <>
-struct Vec16<double> {
-    static constexpr int W = 2;
-    __device__ static void load(const double* p, double* o)
+template <int NQ, int RPT>
+struct RowMat<NQ, RPT, float> {
+    static constexpr int RD = 6 * NQ;
+    float2 v[RPT][RD / 2];
+    __device__ __forceinline__ void load(const float* base, size_t jstride, bool act)
     {
-        const double2 v = *reinterpret_cast<const double2*>(p);
-        o[0] = v.x; o[1] = v.y;
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+            const float2* src = reinterpret_cast<const float2*>(base + j * jstride);
+#pragma unroll
+            for (int c = 0; c < RD / 2; ++c) v[j][c] = act ? src[c] : make_float2(0.f, 0.f);
+        }
     }
 };
 
-// out[j] = row[j] . window for the RPT rows of a thread (three blocks of a
-// padded vector, four partial sums per row)
+// out[j] = row[j] . window for the RPT rows of a thread: three blocks of a
+// vector at stride VS, four partial sums per row by column mod 4, combined
+// as (s0 + s1) + (s2 + s3).
 template <int NQ, int RPT, typename T>
-__device__ __forceinline__ void rows_window_dot(const T (&row)[RPT][3 * 2 * NQ], const T* win,
+__device__ __forceinline__ void rows_window_dot(const RowMat<NQ, RPT, T>& row, const T* win,
                                                 T (&out)[RPT])
 {
-    constexpr int n = 2 * NQ, VS = (n + 3) & ~3, W = Vec16<T>::W;
+    constexpr int n = 2 * NQ, VS = row_vs(n);
+    static_assert(sizeof(T) == 8, "FP32 has its own overload");
     T acc[RPT][4];
 #pragma unroll
     for (int j = 0; j < RPT; ++j)
@@ -547,21 +578,44 @@ __device__ __forceinline__ void rows_window_dot(const T (&row)[RPT][3 * 2 * NQ],
 #pragma unroll
     for (int blk = 0; blk < 3; ++blk) {
 #pragma unroll
-        for (int c0 = 0; c0 < VS; c0 += W) {
-            T v[W];
-            Vec16<T>::load(win + blk * VS + c0, v);
+        for (int c0 = 0; c0 < n; c0 += 2) {
+            const double2 v = *reinterpret_cast<const double2*>(win + blk * VS + c0);
 #pragma unroll
-            for (int w = 0; w < W; ++w) {
-                const int c = c0 + w;
-                if (c < n) {
-#pragma unroll
-                    for (int j = 0; j < RPT; ++j) acc[j][c & 3] += row[j][blk * n + c] * v[w];
-                }
+            for (int j = 0; j < RPT; ++j) {
+                acc[j][c0 & 3] += row.v[j][blk * n + c0] * v.x;
+                acc[j][(c0 + 1) & 3] += row.v[j][blk * n + c0 + 1] * v.y;
             }
         }
     }
 #pragma unroll
     for (int j = 0; j < RPT; ++j) out[j] = (acc[j][0] + acc[j][1]) + (acc[j][2] + acc[j][3]);
+}
+
+template <int NQ, int RPT>
+__device__ __forceinline__ void rows_window_dot(const RowMat<NQ, RPT, float>& row,
+                                                const float* win, float (&out)[RPT])
+{
+    constexpr int n = 2 * NQ, VS = row_vs(n);
+    static_assert(n % 2 == 0, "column pairs");
+    float2 acc[RPT][2];  // (s0, s1), (s2, s3)
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) acc[j][0] = acc[j][1] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int blk = 0; blk < 3; ++blk) {
+#pragma unroll
+        for (int c0 = 0; c0 < n; c0 += 4) {
+            const float4 v = *reinterpret_cast<const float4*>(win + blk * VS + c0);
+            const float2 lo = make_float2(v.x, v.y), hi = make_float2(v.z, v.w);
+#pragma unroll
+            for (int j = 0; j < RPT; ++j) {
+                acc[j][0] = __ffma2_rn(row.v[j][(blk * n + c0) / 2], lo, acc[j][0]);
+                if (c0 + 2 < n) acc[j][1] = __ffma2_rn(row.v[j][(blk * n + c0) / 2 + 1], hi, acc[j][1]);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < RPT; ++j)
+        out[j] = (acc[j][0].x + acc[j][0].y) + (acc[j][1].x + acc[j][1].y);
 }
 
 template <typename Acc>
@@ -621,17 +675,11 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
 #pragma unroll
     for (int j = 0; j < RPT; ++j) x[j] = act ? lam[(k + 1) * n + i0 + j * TPB] : T(0);
     if (!bt.conv[b]) {
-        T srow[RPT][RD], prow[RPT][RD];
-#pragma unroll
-        for (int j = 0; j < RPT; ++j) {
-            const size_t row = (size_t)(k * n + i0 + j * TPB) * RD;
-            const T* Sg = bt.S + (size_t)b * d.b3d() + row;
-            const T* Pg = bt.P + (size_t)b * d.b3d() + row;
-#pragma unroll
-            for (int c = 0; c < RD; ++c) {
-                srow[j][c] = act ? Sg[c] : T(0);
-                prow[j][c] = act ? Pg[c] : T(0);
-            }
+        RowMat<NQ, RPT, T> srow, prow;
+        {
+            const size_t row = (size_t)b * d.b3d() + (size_t)(k * n + i0) * RD;
+            srow.load(bt.S + row, (size_t)TPB * RD, act);
+            prow.load(bt.P + row, (size_t)TPB * RD, act);
         }
         T g[RPT], r[RPT], z[RPT], p[RPT], ap[RPT];
 #pragma unroll
@@ -643,7 +691,7 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
             for (int j = 0; j < RPT; ++j) pv[(k + 1) * VS + i0 + j * TPB] = x[j];
         }
         __syncthreads();
-        rows_window_dot<NQ, RPT, T>(srow, pv + w0, r);
+        rows_window_dot(srow, pv + w0, r);
         Acc part = 0;
 #pragma unroll
         for (int j = 0; j < RPT; ++j) {
@@ -651,7 +699,7 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
             if (act) rv[(k + 1) * VS + i0 + j * TPB] = r[j];
         }
         __syncthreads();
-        rows_window_dot<NQ, RPT, T>(prow, rv + w0, z);
+        rows_window_dot(prow, rv + w0, z);
         const Acc abs_tol = Acc(bt.abs_tol);
         const T eps = bt.tol[b];
         if constexpr (sizeof(T) == 4) {
@@ -666,7 +714,7 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
                 for (int j = 0; j < RPT; ++j) pv[(k + 1) * VS + i0 + j * TPB] = z[j];
             }
             __syncthreads();
-            rows_window_dot<NQ, RPT, T>(srow, pv + w0, w);
+            rows_window_dot(srow, pv + w0, w);
             Acc rho = 0, delta = 0;
 #pragma unroll
             for (int j = 0; j < RPT; ++j) {
@@ -693,13 +741,13 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
                         if (act) rv[(k + 1) * VS + i0 + j * TPB] = r[j];
                     }
                     __syncthreads();
-                    rows_window_dot<NQ, RPT, T>(prow, rv + w0, z);
+                    rows_window_dot(prow, rv + w0, z);
                     if (act) {
 #pragma unroll
                         for (int j = 0; j < RPT; ++j) pv[(k + 1) * VS + i0 + j * TPB] = z[j];
                     }
                     __syncthreads();
-                    rows_window_dot<NQ, RPT, T>(srow, pv + w0, w);
+                    rows_window_dot(srow, pv + w0, w);
                     Acc rho_new = 0;
                     delta = 0;
 #pragma unroll
@@ -742,7 +790,7 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
                         for (int j = 0; j < RPT; ++j) pv[(k + 1) * VS + i0 + j * TPB] = p[j];
                     }
                     __syncthreads();
-                    rows_window_dot<NQ, RPT, T>(srow, pv + w0, ap);
+                    rows_window_dot(srow, pv + w0, ap);
                     part = 0;
 #pragma unroll
                     for (int j = 0; j < RPT; ++j) part += act ? (Acc)p[j] * (Acc)ap[j] : Acc(0);
@@ -756,7 +804,7 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
                         if (act) rv[(k + 1) * VS + i0 + j * TPB] = r[j];
                     }
                     __syncthreads();
-                    rows_window_dot<NQ, RPT, T>(prow, rv + w0, z);
+                    rows_window_dot(prow, rv + w0, z);
                     part = 0;
 #pragma unroll
                     for (int j = 0; j < RPT; ++j) part += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);

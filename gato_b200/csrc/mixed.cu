@@ -43,7 +43,7 @@ void mixed_args(gato_mixed* mx, void* const* xu, const void* const* xs, const vo
 template <typename T>
 bool rows_fit(const gato_solver* s)
 {
-    constexpr int RPT = sizeof(T) == 4 ? 2 : 1;
+    constexpr int RPT = pcg_rows_per_thread<T>();
     return s->nq == 7 ? RowPcg<7, RPT>::fits(s->N) : RowPcg<6, RPT>::fits(s->N);
 }
 
@@ -90,7 +90,7 @@ template <typename T, typename Acc>
 int enqueue_mixed(gato_mixed* mx, cudaStream_t st, void* const* xu, const void* const* xs,
                   const void* const* goal)
 {
-    constexpr int RPT = sizeof(T) == 4 ? 2 : 1;
+    constexpr int RPT = pcg_rows_per_thread<T>();
     MultiArgs<T> ma;
     mixed_args<T, Acc>(mx, xu, xs, goal, ma);
     int nmax = 0, rows_smem = 0;

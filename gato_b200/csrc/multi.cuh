@@ -69,10 +69,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MINB : 1)
 
 // register-resident PCG + step of every queued short-horizon problem
 template <typename T, typename Acc>
-__global__ void __launch_bounds__(RowPcg<7, sizeof(T) == 4 ? 2 : 1>::MAX_THREADS, 1)
+__global__ void __launch_bounds__(RowPcg<7, pcg_rows_per_thread<T>()>::MAX_THREADS, 1)
     k_q_pcg_rows(MultiArgs<T> ma, int it_row)
 {
-    constexpr int RPT = sizeof(T) == 4 ? 2 : 1;
+    constexpr int RPT = pcg_rows_per_thread<T>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_item;
     for (;;) {

@@ -20,7 +20,7 @@ namespace gato {
 
 template <int NQ, int RPT>
 struct ClusterPcg {
-    static constexpr int n = 2 * NQ, m = NQ, RD = 3 * n, VS = (n + 3) & ~3;
+    static constexpr int n = 2 * NQ, m = NQ, RD = 3 * n, VS = row_vs(n);
     static constexpr int TPB = n / RPT;
     static constexpr int MAX_ROWS = 32;    // block rows per CTA
     static constexpr int MAX_CLUSTER = 8;  // portable cluster size
@@ -127,35 +127,29 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
 #pragma unroll
     for (int j = 0; j < RPT; ++j) x[j] = act ? lam[(k + 1) * n + i0 + j * TPB] : T(0);
     if (!bt.conv[b]) {  // per problem: the same on every CTA of the cluster
-        T srow[RPT][RD], prow[RPT][RD];
-#pragma unroll
-        for (int j = 0; j < RPT; ++j) {
-            const size_t row = (size_t)(k * n + i0 + j * TPB) * RD;
-            const T* Sg = bt.S + (size_t)b * d.b3d() + row;
-            const T* Pg = bt.P + (size_t)b * d.b3d() + row;
-#pragma unroll
-            for (int cc = 0; cc < RD; ++cc) {
-                srow[j][cc] = act ? Sg[cc] : T(0);
-                prow[j][cc] = act ? Pg[cc] : T(0);
-            }
+        RowMat<NQ, RPT, T> srow, prow;
+        {
+            const size_t row = (size_t)b * d.b3d() + (size_t)(k * n + i0) * RD;
+            srow.load(bt.S + row, (size_t)TPB * RD, act);
+            prow.load(bt.P + row, (size_t)TPB * RD, act);
         }
         T g[RPT], r[RPT], z[RPT], p[RPT], w[RPT];
 #pragma unroll
         for (int j = 0; j < RPT; ++j)
             g[j] = act ? bt.gamma[(size_t)b * d.vecp() + (k + 1) * n + i0 + j * TPB] : T(0);
         exchange(pv, x);
-        rows_window_dot<NQ, RPT, T>(srow, pv + w0, r);
+        rows_window_dot(srow, pv + w0, r);
 #pragma unroll
         for (int j = 0; j < RPT; ++j) r[j] = act ? g[j] - r[j] : T(0);
         exchange(rv, r);
-        rows_window_dot<NQ, RPT, T>(prow, rv + w0, z);
+        rows_window_dot(prow, rv + w0, z);
         const Acc abs_tol = Acc(bt.abs_tol);
         const T eps = bt.tol[b];
         if constexpr (sizeof(T) == 4) {
             // single-reduction recurrence, as in k_pcg_rows
             T sv[RPT];
             exchange(pv, z);
-            rows_window_dot<NQ, RPT, T>(srow, pv + w0, w);
+            rows_window_dot(srow, pv + w0, w);
             Acc rho = 0, delta = 0;
 #pragma unroll
             for (int j = 0; j < RPT; ++j) {
@@ -181,9 +175,9 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
                         r[j] -= a * sv[j];
                     }
                     exchange(rv, r);
-                    rows_window_dot<NQ, RPT, T>(prow, rv + w0, z);
+                    rows_window_dot(prow, rv + w0, z);
                     exchange(pv, z);
-                    rows_window_dot<NQ, RPT, T>(srow, pv + w0, w);
+                    rows_window_dot(srow, pv + w0, w);
                     Acc rho_new = 0;
                     delta = 0;
 #pragma unroll
@@ -224,7 +218,7 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
                 for (int it = 0; it < bt.max_pcg_iters; ++it) {
                     ++iters;
                     exchange(pv, p);
-                    rows_window_dot<NQ, RPT, T>(srow, pv + w0, w);
+                    rows_window_dot(srow, pv + w0, w);
                     Acc pap = 0;
                     unused = 0;
 #pragma unroll
@@ -238,7 +232,7 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
                         r[j] -= alpha * w[j];
                     }
                     exchange(rv, r);
-                    rows_window_dot<NQ, RPT, T>(prow, rv + w0, z);
+                    rows_window_dot(prow, rv + w0, z);
                     Acc rho_new = 0;
                     unused = 0;
 #pragma unroll

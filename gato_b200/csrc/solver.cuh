@@ -460,6 +460,19 @@ int launch_ls(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::
     return GATO_OK;
 }
 
+// register-resident PCG + dz of every problem, one CTA each
+template <class Tg>
+void launch_pcg_rows(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt,
+                     int row)
+{
+    constexpr int NQ = Tg::NQ;
+    using T = typename Tg::T;
+    using Acc = typename Tg::Acc;
+    constexpr int RPT = pcg_rows_per_thread<T>();
+    k_pcg_rows<NQ, T, Acc, RPT><<<s->B, RowPcg<NQ, RPT>::threads(s->N),
+                                   RowPcg<NQ, RPT>::template smem_bytes<T>(s->N), st>>>(bt, row);
+}
+
 // cluster PCG + step for horizons beyond one CTA's registers (N > ~36)
 template <class Tg>
 int launch_pcg_cluster(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt,
@@ -468,7 +481,7 @@ int launch_pcg_cluster(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, type
     constexpr int NQ = Tg::NQ;
     using T = typename Tg::T;
     using Acc = typename Tg::Acc;
-    constexpr int RPT = sizeof(T) == 4 ? 2 : 1;
+    constexpr int RPT = pcg_rows_per_thread<T>();
     using CP = ClusterPcg<NQ, RPT>;
     ProfScope ps_(s, st, GATO_KERNEL_PCG);
     const int C = CP::ctas(s->N);
@@ -497,7 +510,7 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
     using Acc = typename Tg::Acc;
     // rows of S and P^-1 per thread in k_pcg_rows: two in FP32 (each window
     // value loaded from shared memory feeds two rows), one in FP64 (registers)
-    constexpr int RPT = sizeof(T) == 4 ? 2 : 1;
+    constexpr int RPT = pcg_rows_per_thread<T>();
     // Fewer problems than half the SMs: one CTA per problem would leave SMs
     // idle and make every problem's KKT blocks a serial chain of knots, so
     // the KKT runs knot-parallel (k_kkt, a warp per knot) and the fused
@@ -515,9 +528,7 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
             CKL();
         }
         ProfScope ps2_(s, st, GATO_KERNEL_PCG);
-        k_pcg_rows<NQ, T, Acc, RPT><<<s->B, RowPcg<NQ, RPT>::threads(s->N),
-                                       RowPcg<NQ, RPT>::template smem_bytes<T>(s->N), st>>>(bt,
-                                                                                            row);
+        launch_pcg_rows<Tg>(s, st, bt, row);
         CKL();
         return GATO_OK;
     }
@@ -577,7 +588,7 @@ int configure_kernels(gato_solver* s)
         return fail(GATO_ERR_UNSUPPORTED, "N=%d needs %zu bytes of shared memory", s->N,
                     lay.bytes());
     RC(set_smem(k_fused_iter<NQ, T, Acc>, lay.bytes(), s->max_smem));
-    constexpr int RPT = sizeof(T) == 4 ? 2 : 1;
+    constexpr int RPT = pcg_rows_per_thread<T>();
     RC(set_smem(k_pcg_rows<NQ, T, Acc, RPT>, RowPcg<NQ, RPT>::template smem_bytes<T>(s->N),
                 s->max_smem));
     return GATO_OK;
@@ -775,12 +786,10 @@ int pcg_and_step(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename T
     constexpr int NQ = Tg::NQ;
     using T = typename Tg::T;
     using Acc = typename Tg::Acc;
-    constexpr int RPT = sizeof(T) == 4 ? 2 : 1;
+    constexpr int RPT = pcg_rows_per_thread<T>();
     if (RowPcg<NQ, RPT>::fits(s->N)) {
         ProfScope ps_(s, st, GATO_KERNEL_PCG);
-        k_pcg_rows<NQ, T, Acc, RPT><<<s->B, RowPcg<NQ, RPT>::threads(s->N),
-                                       RowPcg<NQ, RPT>::template smem_bytes<T>(s->N), st>>>(bt,
-                                                                                            -1);
+        launch_pcg_rows<Tg>(s, st, bt, -1);
         CKL();
         return GATO_OK;
     }
