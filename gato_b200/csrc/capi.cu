@@ -96,6 +96,7 @@ int gato_create(const gato_model_t* model, int N, int batch, const gato_params_t
     RC(p->alloc(&p->conv, B));
     RC(p->alloc(&p->sqp_iters, B));
     RC(p->alloc(&p->done, 1));
+    RC(p->alloc(&p->work, 4));
     RC(p->alloc(&p->ls_count, 1));
     RC(p->alloc(&p->h_pcg, (size_t)iters * B));
     RC(p->alloc(&p->h_ls_min, (size_t)iters * B));
@@ -232,7 +233,7 @@ int gato_profile_solve(gato_solver_t* s, void* stream, float* d_xu, const float*
     }
     if (rc) return rc;
     if (e != cudaSuccess) return fail(GATO_ERR_CUDA, "profile solve: %s", cudaGetErrorString(e));
-    return GATO_OK;
+    return check_device_waits(s);
 }
 
 int gato_set_f_ext_batch(gato_solver_t* s, const float* h_f_ext)

@@ -8,6 +8,8 @@
 // stays on the device so that a whole solve is one CUDA graph.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "dynamics.cuh"
 #include "dynamics_thread.cuh"
@@ -39,6 +41,9 @@ struct Batch {
     double *merit_init, *merit_init0, *merit_final;
     int *pcg_iters, *conv, *sqp_iters;
     int* done;             // device flag: batch converged (fused form)
+    // [0] next problem of a persistent launch, [1] CTAs finished, [2] a
+    // bounded wait expired (both counters are back at 0 after each launch)
+    int* work;
     int* ls_count;         // line-search iterations run (fused form)
     // per-iteration statistics [iter][B]
     int* h_pcg;
@@ -651,10 +656,19 @@ __device__ __forceinline__ void rows_block_sum2(Acc& a, Acc& b, Acc* red)
     b = sb;
 }
 
-template <int NQ, typename T, typename Acc, int RPT>
+struct NoHook {
+    __device__ void operator()() const {}
+};
+
+// Sp, Pp: the problem's S and P^-1 (row-major [N n][3n]) in global or shared
+// memory (null: bt.S, bt.P).  hook() runs on every thread after the CG loop,
+// behind a barrier: Sp and Pp are no longer read.
+template <int NQ, typename T, typename Acc, int RPT, class Hook = NoHook>
 __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int it_row,
-                                              unsigned char* smem_raw)
+                                              unsigned char* smem_raw, const T* Sp = nullptr,
+                                              const T* Pp = nullptr, Hook hook = Hook())
 {
+    constexpr bool HOOK = !std::is_same<Hook, NoHook>::value;
     using RP = RowPcg<NQ, RPT>;
     constexpr int n = RP::n, m = RP::m, RD = RP::RD, VS = RP::VS, TPB = RP::TPB;
     if (*bt.done) return;
@@ -677,9 +691,10 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
     if (!bt.conv[b]) {
         RowMat<NQ, RPT, T> srow, prow;
         {
-            const size_t row = (size_t)b * d.b3d() + (size_t)(k * n + i0) * RD;
-            srow.load(bt.S + row, (size_t)TPB * RD, act);
-            prow.load(bt.P + row, (size_t)TPB * RD, act);
+            const size_t row = (size_t)(k * n + i0) * RD;
+            const size_t prob = (size_t)b * d.b3d();
+            srow.load((Sp ? Sp : bt.S + prob) + row, (size_t)TPB * RD, act);
+            prow.load((Pp ? Pp : bt.P + prob) + row, (size_t)TPB * RD, act);
         }
         T g[RPT], r[RPT], z[RPT], p[RPT], ap[RPT];
 #pragma unroll
@@ -827,6 +842,7 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
     // res_x = q_k - lambda_k + A_k^T lambda_{k+1}, dz_x = -Qi_k res_x,
     // res_u = r_k + B_k^T lambda_{k+1}, dz_u = -Ri_k res_u
     __syncthreads();
+    if constexpr (HOOK) hook();
     if (act) {
 #pragma unroll
         for (int j = 0; j < RPT; ++j) pv[(k + 1) * VS + i0 + j * TPB] = x[j];
@@ -903,6 +919,90 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     pcg_rows_body<NQ, T, Acc, RPT>(bt, blockIdx.x, it_row, smem_raw);
+}
+
+// Persistent FP32 form of k_pcg_rows: one CTA per SM takes problems from a
+// counter (bt.work[0]).  When a problem's CG loop ends, the CTA claims the
+// next problem and the bulk-copy engine brings its S and P^-1 (2 x 12 N NQ^2
+// floats, contiguous per problem) into shared memory while the CTA computes
+// the step dz, so the matrices load from shared memory instead of as strided
+// rows from HBM.  Claiming at the end rather than the start of a problem
+// keeps the assignment as adaptive as the hardware's block scheduling (the
+// early claim cost the adjoint's long, uneven CG runs 8 %).  Per-problem arithmetic is that of
+// k_pcg_rows.  Thread 0 alone waits on the copy's mbarrier, with a bound;
+// the outcome goes through shared memory so that every thread takes the same
+// branch.  An expired wait sets bt.work[2] and ends the CTA.
+template <int NQ>
+struct PcgStage {
+    __host__ __device__ static size_t matrix_floats(int N) { return (size_t)12 * N * NQ * NQ; }
+    __host__ __device__ static size_t offset(int N)
+    {
+        return (RowPcg<NQ, 2>::template smem_bytes<float>(N) + 127) & ~(size_t)127;
+    }
+    __host__ __device__ static size_t smem_bytes(int N)
+    {
+        return offset(N) + 2 * matrix_floats(N) * sizeof(float);
+    }
+};
+
+constexpr int PCG_STAGE_WAIT_TRIES = 1 << 22;
+
+template <int NQ, typename Acc>
+__global__ void __launch_bounds__(RowPcg<NQ, 2>::MAX_THREADS, 1)
+    k_pcg_rows_stream(Batch<NQ, float> bt, int it_row)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int s_next, s_ok;
+    if (*bt.done) return;
+    const int N = bt.N, B = bt.B, tid = threadIdx.x;
+    const size_t mat = PcgStage<NQ>::matrix_floats(N);
+    float* stS = reinterpret_cast<float*>(smem_raw + PcgStage<NQ>::offset(N));
+    float* stP = stS + mat;
+    const uint32_t bytes = (uint32_t)(mat * sizeof(float));
+    auto fetch = [&](int pb) {  // thread 0; earlier reads of the stage are behind a barrier
+        fence_proxy_async_shared();
+        mbar_arrive_expect_tx(&bar, 2 * bytes);
+        bulk_copy_g2s(stS, bt.S + (size_t)pb * mat, bytes, &bar);
+        bulk_copy_g2s(stP, bt.P + (size_t)pb * mat, bytes, &bar);
+    };
+    int b = blockIdx.x;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+        if (b < B) fetch(b);
+    }
+    uint32_t parity = 0;
+    while (b < B) {
+        __syncthreads();  // the previous problem is done with the vectors and s_next
+        if (tid == 0) {
+            int i = 0;
+            while (!mbar_try_wait(&bar, parity) && ++i < PCG_STAGE_WAIT_TRIES) {
+            }
+            s_ok = i < PCG_STAGE_WAIT_TRIES;
+        }
+        __syncthreads();
+        if (!s_ok) {
+            if (tid == 0) atomicExch(bt.work + 2, 1);
+            break;
+        }
+        if (tid != 0) mbar_try_wait(&bar, parity);  // phase complete: acquires the data
+        parity ^= 1;
+        auto next = [&]() {
+            if (tid == 0) {
+                const int nb = (int)gridDim.x + atomicAdd(bt.work, 1);
+                s_next = nb;
+                if (nb < B) fetch(nb);
+            }
+        };
+        pcg_rows_body<NQ, float, Acc, 2>(bt, b, it_row, smem_raw, stS, stP, next);
+        __syncthreads();
+        b = s_next;
+    }
+    if (tid == 0 && atomicAdd(bt.work + 1, 1) == (int)gridDim.x - 1) {
+        bt.work[0] = 0;  // last CTA out: ready for the next launch
+        bt.work[1] = 0;
+    }
 }
 
 // ------------------------------------------------------------------ dz

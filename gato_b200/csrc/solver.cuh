@@ -147,12 +147,14 @@ void build_dev_model(const gato_model_t& m, DevModel<NQ, T>* out)
 template <class K>
 int set_smem(K kernel, size_t bytes, int device_limit)
 {
-    if (bytes > (size_t)device_limit)
+    cudaFuncAttributes fa{};
+    CK(cudaFuncGetAttributes(&fa, kernel));
+    const int dyn_limit = device_limit - (int)fa.sharedSizeBytes;  // minus static shared memory
+    if (bytes > (size_t)dyn_limit)
         return fail(GATO_ERR_UNSUPPORTED, "kernel needs %zu bytes of shared memory, device has %d",
-                    bytes, device_limit);
+                    bytes, dyn_limit);
     if (bytes > 48 * 1024)
-        CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                device_limit));
+        CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_limit));
     return GATO_OK;
 }
 
@@ -190,6 +192,7 @@ struct gato_solver {
            *merit_final = nullptr;
     int *pcg_iters = nullptr, *conv = nullptr, *sqp_iters = nullptr, *done = nullptr,
         *ls_count = nullptr, *h_pcg = nullptr;
+    int* work = nullptr;  // [4]: counters and wait flag of the persistent PCG
     float *h_ls_min = nullptr, *h_ls_step = nullptr;
     // adjoint work buffers, allocated by the first gato_adjoint call
     void *adj_lam = nullptr, *adj_mu = nullptr, *adj_v = nullptr, *adj_scale = nullptr,
@@ -316,6 +319,7 @@ Batch<Tg::NQ, typename Tg::T> make_batch(gato_solver* s, void* xu, const void* x
     b.conv = s->conv;
     b.sqp_iters = s->sqp_iters;
     b.done = s->done;
+    b.work = s->work;
     b.ls_count = s->ls_count;
     b.h_pcg = s->h_pcg;
     b.h_ls_min = s->h_ls_min;
@@ -460,7 +464,19 @@ int launch_ls(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::
     return GATO_OK;
 }
 
-// register-resident PCG + dz of every problem, one CTA each
+// FP32 runs the persistent k_pcg_rows_stream (one CTA per SM, the next
+// problem's matrices prefetched into shared memory) when its stage fits
+template <class Tg>
+bool pcg_stream_fits(const gato_solver* s)
+{
+    if constexpr (sizeof(typename Tg::T) == 4)
+        return RowPcg<Tg::NQ, 2>::fits(s->N) &&
+               PcgStage<Tg::NQ>::smem_bytes(s->N) + 64 <= (size_t)s->max_smem;
+    else
+        return false;
+}
+
+// register-resident PCG + dz of every problem
 template <class Tg>
 void launch_pcg_rows(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt,
                      int row)
@@ -468,6 +484,14 @@ void launch_pcg_rows(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typena
     constexpr int NQ = Tg::NQ;
     using T = typename Tg::T;
     using Acc = typename Tg::Acc;
+    if constexpr (sizeof(T) == 4) {
+        if (pcg_stream_fits<Tg>(s)) {
+            const int grid = std::min(s->B, s->nsm);
+            k_pcg_rows_stream<NQ, Acc><<<grid, RowPcg<NQ, 2>::threads(s->N),
+                                         PcgStage<NQ>::smem_bytes(s->N), st>>>(bt, row);
+            return;
+        }
+    }
     constexpr int RPT = pcg_rows_per_thread<T>();
     k_pcg_rows<NQ, T, Acc, RPT><<<s->B, RowPcg<NQ, RPT>::threads(s->N),
                                    RowPcg<NQ, RPT>::template smem_bytes<T>(s->N), st>>>(bt, row);
@@ -591,6 +615,10 @@ int configure_kernels(gato_solver* s)
     constexpr int RPT = pcg_rows_per_thread<T>();
     RC(set_smem(k_pcg_rows<NQ, T, Acc, RPT>, RowPcg<NQ, RPT>::template smem_bytes<T>(s->N),
                 s->max_smem));
+    if constexpr (sizeof(T) == 4) {
+        if (pcg_stream_fits<Tg>(s))
+            RC(set_smem(k_pcg_rows_stream<NQ, Acc>, PcgStage<NQ>::smem_bytes(s->N), s->max_smem));
+    }
     return GATO_OK;
 }
 
@@ -699,8 +727,22 @@ int solve_fused(gato_solver* s, cudaStream_t st, void* xu, const void* xs, const
     return GATO_OK;
 }
 
+// Reports (and clears) an expired bounded wait in a device kernel.  The
+// caller has synchronised the solver's stream.
+int check_device_waits(gato_solver* s)
+{
+    int flag = 0;
+    CK(cudaMemcpy(&flag, s->work + 2, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        CK(cudaMemset(s->work + 2, 0, sizeof(int)));
+        return fail(GATO_ERR_TIMEOUT, "PCG: the wait for a problem's matrices in shared memory expired");
+    }
+    return GATO_OK;
+}
+
 int read_stats(gato_solver* s, const int* hsqp, const int* hconv, int rows, gato_stats_t* stats)
 {
+    RC(check_device_waits(s));
     const int B = s->B;
     const int iters = std::max(1, s->params.max_sqp_iters);
     float ms = 0.0f;
