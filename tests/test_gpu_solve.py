@@ -225,3 +225,25 @@ def test_interface_drop_in_surface():
     p = s.ee_pos(pr["xs"][0][:6])
     assert p.shape == (3,)
     s.close()
+
+
+@pytest.mark.parametrize("B", [5, 149, 300])
+def test_fused_solve_repeats_exactly(B):
+    """The FP32 fused form's PCG runs persistently (one CTA per SM taking
+    problems from a device counter that each launch leaves at zero): a batch
+    smaller than the SM count, one just above it and one of about two rounds
+    are solved twice from the same state; every problem ran its PCG and the
+    second solve repeats the first bit for bit."""
+    pr = problem("iiwa14", 32, B, seed=17)
+    s = gpu_solver("iiwa14", 32, B, form="fused", precision="fp32", **PARAMS_CFG2)
+    lam0 = s.get_lambda()
+    outs = []
+    for _ in range(2):
+        s.set_lambda(lam0)
+        s.reset_rho()
+        outs.append(s.solve_raw(pr["xu"], 0.01, pr["xs"], pr["goal"]))
+    s.close()
+    a, b = outs
+    assert (a["pcg_iters"][0] > 0).all()
+    np.testing.assert_array_equal(a["XU"], b["XU"])
+    np.testing.assert_array_equal(a["pcg_iters"], b["pcg_iters"])
