@@ -238,8 +238,32 @@ def cpu_baseline(wl, sample, threads, with_result=False):
                      wl["xs"][:sample].astype(np.float64), wl["goal"][:sample].astype(np.float64))
     dt = time.perf_counter() - t0
     if with_result:
+        so = dict(so, lam=S.get_lambda())
         return sample / dt, dt, xo, so
     return sample / dt, dt
+
+
+def kkt_measures(xu, lam, xs, goal):
+    """Per problem, at trajectory xu with multipliers lam (padded [(N+2) nx]),
+    from the FP64 oracle's KKT blocks: the dynamics defect max|c| (c_0 =
+    x_0 - x_s, c_{k+1} the integrator defect) and the KKT stationarity
+    max|grad L|, the residuals of the reference's step recovery
+    (schur_linsys.cuh:312-431): q_k - lam_k + A_k^T lam_{k+1} and
+    r_k + B_k^T lam_{k+1}."""
+    from oracle import oracle as O
+    P = O.make_params(dt=DT, **solver_kwargs())
+    model = O.Model(PLANT)
+    n = 2 * model.nq
+    defect, stat = [], []
+    for b in range(xu.shape[0]):
+        kb = model.setup_kkt(N, P, DT, xu[b], xs[b], goal[b])
+        lk = lam[b].reshape(N + 2, n)[1:N + 1]
+        res = [kb["q"][k] - lk[k] + (kb["A"][k] @ lk[k + 1] if k < N - 1 else 0.0)
+               for k in range(N)]
+        res += [kb["r"][k] + kb["B"][k] @ lk[k + 1] for k in range(N - 1)]
+        defect.append(float(np.abs(kb["c"]).max()))
+        stat.append(float(max(np.abs(v).max() for v in res)))
+    return np.array(defect), np.array(stat)
 
 
 def run_reference(args):
@@ -556,12 +580,29 @@ def run_ours(args):
         torch.cuda.synchronize()
         xg = d_xu.double().cpu().numpy()[:sample]
         errs = np.abs(xg - xo).max(axis=1) / np.maximum(1.0, np.abs(xo).max(axis=1))
+        ks = min(sample, 64)
+        xs64, goal64 = wl["xs"][:ks].astype(np.float64), wl["goal"][:ks].astype(np.float64)
+        dg, sg = kkt_measures(xg[:ks], fused.get_lambda()[:ks].astype(np.float64), xs64, goal64)
+        do, so_ = kkt_measures(xo[:ks], so["lam"][:ks], xs64, goal64)
         accuracy = {"sample": sample, "xu_rel_err_max": float(errs.max()),
                     "xu_rel_err_median": float(np.median(errs)),
                     "pcg_iters_equal_frac": float(np.mean(
                         stg["pcg_iters"][:, :sample] == so["pcg_iters"]))
                     if stg["pcg_iters"].shape[0] == so["pcg_iters"].shape[0] else None,
-                    "note": "FP32 fused solve vs the FP64 oracle of the same SQP, same inputs"}
+                    "dynamics_defect": {"problems": ks, "median": float(np.median(dg)),
+                                        "max": float(dg.max()),
+                                        "oracle_median": float(np.median(do)),
+                                        "oracle_max": float(do.max()),
+                                        "rel_diff_median": float(np.median(
+                                            np.abs(dg - do) / np.maximum(do, 1e-12)))},
+                    "kkt_stationarity": {"problems": ks, "median": float(np.median(sg)),
+                                         "max": float(sg.max()),
+                                         "oracle_median": float(np.median(so_)),
+                                         "oracle_max": float(so_.max()),
+                                         "rel_diff_median": float(np.median(
+                                             np.abs(sg - so_) / np.maximum(so_, 1e-12)))},
+                    "note": "FP32 fused solve vs the FP64 oracle of the same SQP, same inputs; "
+                            "defect and stationarity from FP64 KKT blocks at each result"}
     if dist:
         dist.destroy_process_group()
     if rank != 0:
