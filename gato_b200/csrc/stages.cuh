@@ -203,24 +203,33 @@ __device__ __forceinline__ void warp_invert(const T* src, T rho_half, T* dst)
 }
 
 // out (m x n) = A (m x kdim) * B (kdim x n) [+ C if accumulate]; column-major,
-// leading dimensions equal to the row counts; lane j computes column j.
-// transB selects B^T (B stored n x kdim).
+// leading dimensions equal to the row counts.  Lane j of each half-warp
+// computes column j: the lower half-warp rows [0, R0), the upper [R0, MR), so
+// 2 NC lanes share the work (one column per lane would leave more than half
+// of the warp idle at NC = 14).  Every entry is the same FMA sequence over t
+// as with one lane per column.  transB selects B^T (B stored n x kdim).
 template <int MR, int KD, int NC, bool TRANSB, bool ACC, typename T>
 __device__ __forceinline__ void warp_gemm(T* out, const T* A, const T* B)
 {
+    static_assert(NC <= 16, "one column per lane of a half-warp");
+    constexpr int R0 = (MR + 1) / 2;
     const int l = lane_id();
-    if (l < NC) {
-        T acc[MR];
+    const int j = l & 15, r0 = (l >> 4) ? R0 : 0;
+    if (j < NC) {
+        T acc[R0];
 #pragma unroll
-        for (int r = 0; r < MR; ++r) acc[r] = ACC ? out[l * MR + r] : T(0.0);
+        for (int i = 0; i < R0; ++i)
+            acc[i] = (ACC && r0 + i < MR) ? out[j * MR + r0 + i] : T(0.0);
 #pragma unroll
         for (int t = 0; t < KD; ++t) {
-            const T b = TRANSB ? B[t * NC + l] : B[l * KD + t];
+            const T b = TRANSB ? B[t * NC + j] : B[j * KD + t];
 #pragma unroll
-            for (int r = 0; r < MR; ++r) acc[r] += A[t * MR + r] * b;
+            for (int i = 0; i < R0; ++i)
+                if (MR % 2 == 0 || r0 + i < MR) acc[i] += A[t * MR + r0 + i] * b;
         }
 #pragma unroll
-        for (int r = 0; r < MR; ++r) out[l * MR + r] = acc[r];
+        for (int i = 0; i < R0; ++i)
+            if (MR % 2 == 0 || r0 + i < MR) out[j * MR + r0 + i] = acc[i];
     }
     __syncwarp();
 }
