@@ -276,6 +276,7 @@ __global__ void k_kkt(Batch<NQ, T> bt, DevModel<NQ, T> M)
 template <int NQ, typename T>
 __global__ void k_schur_inv(Batch<NQ, T> bt)
 {
+    if (*bt.done) return;  // fused form: the batch has converged
     const int b = blockIdx.y;
     const int wpb = blockDim.x / WARP;
     const int k = blockIdx.x * wpb + warp_id();
@@ -294,6 +295,7 @@ __global__ void k_schur(Batch<NQ, T> bt)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
+    if (*bt.done) return;
     const int b = blockIdx.y;
     const int wpb = blockDim.x / WARP;
     const int k = blockIdx.x * wpb + warp_id();
@@ -321,6 +323,7 @@ __global__ void k_schur_off(Batch<NQ, T> bt)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
+    if (*bt.done) return;
     const int b = blockIdx.y;
     const int wpb = blockDim.x / WARP;
     const int k = blockIdx.x * wpb + warp_id();

@@ -535,21 +535,24 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
     // rows of S and P^-1 per thread in k_pcg_rows: two in FP32 (each window
     // value loaded from shared memory feeds two rows), one in FP64 (registers)
     constexpr int RPT = pcg_rows_per_thread<T>();
-    // Fewer problems than half the SMs: one CTA per problem would leave SMs
-    // idle and make every problem's KKT blocks a serial chain of knots, so
-    // the KKT runs knot-parallel (k_kkt, a warp per knot) and the fused
-    // kernel starts at the Schur complement (measured: B = 1 and 32 gain
-    // 15-18 %, B = 128 loses 5 %).
-    const int with_kkt = 2 * s->B > s->nsm;
+    // Up to 1.5 problems per SM, one CTA per problem would leave SMs idle
+    // and make every problem's KKT blocks and Schur complement serial chains
+    // of knots, so both run knot-parallel, a warp per knot (k_kkt, then the
+    // plain form's k_schur_inv, k_schur, k_schur_off).  Measured, iiwa14
+    // N = 32, solves/s fused -> split: B = 1 1,020 -> 1,372; B = 96 75.0K ->
+    // 90.7K; B = 192 110.2K -> 113.2K; B = 256 125.6K -> 116.8K.
+    const int with_kkt = 2 * s->B > 3 * s->nsm;
     if (!with_kkt) RC(launch_kkt<Tg>(s, st, bt));
     if (RowPcg<NQ, RPT>::fits(s->N)) {
         // KKT + Schur into global memory, then the register-resident PCG + dz
-        {
+        if (with_kkt) {
             ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
             FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, false};
             k_fused_iter<NQ, T, Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(
-                bt, dmodel<Tg>(s), 0, row, 0, with_kkt);
+                bt, dmodel<Tg>(s), 0, row, 0, 1);
             CKL();
+        } else {
+            RC(launch_schur<Tg>(s, st, bt));
         }
         ProfScope ps2_(s, st, GATO_KERNEL_PCG);
         launch_pcg_rows<Tg>(s, st, bt, row);
@@ -557,12 +560,14 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
         return GATO_OK;
     }
     if (ClusterPcg<NQ, RPT>::fits(s->N)) {
-        {
+        if (with_kkt) {
             ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
             FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, false};
             k_fused_iter<NQ, T, Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(
-                bt, dmodel<Tg>(s), 0, row, 0, with_kkt);
+                bt, dmodel<Tg>(s), 0, row, 0, 1);
             CKL();
+        } else {
+            RC(launch_schur<Tg>(s, st, bt));
         }
         return launch_pcg_cluster<Tg>(s, st, bt, row);
     }
