@@ -227,15 +227,17 @@ def test_interface_drop_in_surface():
     s.close()
 
 
-@pytest.mark.parametrize("B", [5, 149, 300])
-def test_fused_solve_repeats_exactly(B):
+@pytest.mark.parametrize("plant,precision,B", [("iiwa14", "fp32", 5), ("iiwa14", "fp32", 149),
+                                                ("iiwa14", "fp32", 300), ("indy7", "fp32", 149),
+                                                ("iiwa14", "mixed", 149)])
+def test_fused_solve_repeats_exactly(plant, precision, B):
     """The FP32 fused form's PCG runs persistently (one CTA per SM taking
     problems from a device counter that each launch leaves at zero): a batch
     smaller than the SM count, one just above it and one of about two rounds
     are solved twice from the same state; every problem ran its PCG and the
     second solve repeats the first bit for bit."""
-    pr = problem("iiwa14", 32, B, seed=17)
-    s = gpu_solver("iiwa14", 32, B, form="fused", precision="fp32", **PARAMS_CFG2)
+    pr = problem(plant, 32, B, seed=17)
+    s = gpu_solver(plant, 32, B, form="fused", precision=precision, **PARAMS_CFG2)
     lam0 = s.get_lambda()
     outs = []
     for _ in range(2):
