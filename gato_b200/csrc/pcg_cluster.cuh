@@ -189,7 +189,8 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
                     const Acc arn = rho_new < 0 ? -rho_new : rho_new;
                     if (arn < abs_tol + (Acc)eps * rho_init || !(arn > 0)) break;
                     const Acc beta = rho_new / rho;
-                    alpha = rho_new / (delta - beta * rho_new / alpha);
+                    const Acc rn_a = rho_new / alpha;  // independent of beta's division
+                    alpha = rho_new / (delta - beta * rn_a);
                     if (!isfinite((double)alpha)) break;  // breakdown: keep the iterate
                     rho = rho_new;
                     const T bb = (T)beta;

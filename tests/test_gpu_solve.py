@@ -117,8 +117,13 @@ def test_fp32_stepwise_parity_n32(oracle_mod):
     """iiwa14 N=32 (the benchmark configuration), batch 8: five SQP
     iterations, each run once on the GPU (FP32) and once in the oracle (FP64)
     from the identical state (XU, lambda, rho).  FP32 tolerance: at least 85%
-    of the (problem, iteration) PCG counts equal and all within 15%; where the
-    step matches, XU within 5e-3 (normalised) with a median within 1e-3.
+    of the (problem, iteration) PCG counts equal and all within 15%, or, where
+    the oracle's own stop is marginal, between the oracle's counts at half and
+    at twice the tolerance from the same state (one problem here stops at 72
+    iterations in FP64 with |r.z| at 0.5-0.8 of the threshold and needs 152
+    below it; float32 rounding of the recurrence moves |r.z| across it for a
+    third to a half of the summation orders); where the step matches, XU
+    within 5e-3 (normalised) with a median within 1e-3.
     The bound comes from the PCG stopping rule, not from FP32 alone:
     |r.z| < 1e-6 + 1e-5 |r0.z0| leaves a preconditioned residual of about
     sqrt(1e-5) = 3e-3 of the initial one, so two solves that round differently
@@ -143,7 +148,18 @@ def test_fp32_stepwise_parity_n32(oracle_mod):
         pg, po = g["pcg_iters"].ravel(), so["pcg_iters"].ravel()
         eq += int(np.sum(pg == po))
         tot += pg.size
-        assert np.all(np.abs(pg - po) <= np.maximum(2, 0.15 * po)), (pg, po)
+        ok = np.abs(pg - po) <= np.maximum(2, 0.15 * po)
+        if not ok.all():
+            bounds = []
+            for tol in (2.0 * params["pcg_tol"], 0.5 * params["pcg_tol"]):
+                ref.set_lambda(lam.astype(np.float64))
+                ref.set_rho_penalty_batch(rho.astype(np.float64), False)
+                ref.set_pcg_tol_batch(np.full(B, tol))
+                bounds.append(ref.solve(xu.astype(np.float64), 0.01, pr["xs"],
+                                        pr["goal"])[1]["pcg_iters"].ravel())
+            ref.set_pcg_tol_batch(np.full(B, params["pcg_tol"]))
+            lo, hi = bounds
+            assert np.all(ok | ((pg >= lo - 2) & (pg <= hi + 2))), (pg, po, lo, hi)
         same = g["ls_step_size"].ravel() == so["ls_step_size"].ravel().astype(np.float32)
         for b in np.nonzero(same)[0]:
             errs.append(nerr(g["XU"][b], xo[b]))
