@@ -790,7 +790,9 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
                     const Acc beta = rho_new / rho;
                     const Acc rn_a = rho_new / alpha;  // independent of beta's division
                     alpha = rho_new / (delta - beta * rn_a);
-                    if (!isfinite((double)alpha)) break;  // breakdown: keep the iterate
+                    // breakdown: keep the iterate (tested in Acc, no conversion on the
+                    // loop's critical path)
+                    if (!isfinite(alpha)) break;
                     rho = rho_new;
                     const T bb = (T)beta;
 #pragma unroll
