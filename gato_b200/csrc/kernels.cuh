@@ -968,7 +968,7 @@ template <int NQ, typename Acc>
 __global__ void __launch_bounds__(RowPcg<NQ, 2>::MAX_THREADS, 1)
     k_pcg_rows_stream(Batch<NQ, float> bt, int it_row)
 {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];  // stage offset 128-aligned
     __shared__ __align__(8) uint64_t bar;
     __shared__ int s_next, s_ok;
     if (*bt.done) return;

@@ -212,6 +212,37 @@ template <int MR, int KD, int NC, bool TRANSB, bool ACC, typename T>
 __device__ __forceinline__ void warp_gemm(T* out, const T* A, const T* B)
 {
     static_assert(NC <= 16, "one column per lane of a half-warp");
+    if constexpr (sizeof(T) == 4 && MR % 2 == 0) {
+        // FP32: row pairs in packed FMAs (each entry still one fmaf per t, in
+        // order), the lower half-warp taking the first R0 rows, R0 even so
+        // that every pair is an aligned float2 (A and out 8-byte aligned)
+        constexpr int R0 = ((MR / 2) + 1) & ~1, P0 = R0 / 2;
+        const int l = lane_id();
+        const int j = l & 15, hi = l >> 4;
+        const int r0 = hi ? R0 : 0, np = hi ? (MR - R0) / 2 : P0;
+        if (j < NC) {
+            float2 acc[P0];
+#pragma unroll
+            for (int q = 0; q < P0; ++q)
+                acc[q] = (ACC && q < np) ? *reinterpret_cast<const float2*>(out + j * MR + r0 + 2 * q)
+                                         : make_float2(0.f, 0.f);
+#pragma unroll
+            for (int t = 0; t < KD; ++t) {
+                const float b = TRANSB ? B[t * NC + j] : B[j * KD + t];
+                const float2 bb = make_float2(b, b);
+#pragma unroll
+                for (int q = 0; q < P0; ++q)
+                    if (q < np)
+                        acc[q] = __ffma2_rn(
+                            *reinterpret_cast<const float2*>(A + t * MR + r0 + 2 * q), bb, acc[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < P0; ++q)
+                if (q < np) *reinterpret_cast<float2*>(out + j * MR + r0 + 2 * q) = acc[q];
+        }
+        __syncwarp();
+        return;
+    }
     constexpr int R0 = (MR + 1) / 2;
     const int l = lane_id();
     const int j = l & 15, r0 = (l >> 4) ? R0 : 0;
@@ -249,11 +280,11 @@ struct SchurSmem {
     static constexpr int QI = B + n * m;
     static constexpr int QI1 = QI + n2;
     static constexpr int RI = QI1 + n2;
-    static constexpr int PHI = RI + m * m;
+    static constexpr int PHI = RI + ((m * m + 1) & ~1);  // even offsets: float2 operands
     static constexpr int BRI = PHI + n2;
     static constexpr int TH = BRI + n * m;
     static constexpr int V = TH + n2;   // q_k, q_{k+1}, r_k, c_{k+1}
-    static constexpr int SIZE = V + 3 * n + m;
+    static constexpr int SIZE = (V + 3 * n + m + 1) & ~1;
 };
 
 template <int NQ, typename T>
