@@ -38,7 +38,7 @@ PLANT, N, DT = "iiwa14", 32, 0.01
 # DRAM bytes (read + write) per launch from one ncu capture of the first SQP
 # iteration of this workload (profiles/k_fused_iter_iiwa14_N32_B1024.md,
 # profiles/k_pcg_rows_stream_iiwa14_N32_B1024.md)
-TRAFFIC_PER_LAUNCH = {"fused_iter": 923_071_744, "pcg": 239_042_560}
+TRAFFIC_PER_LAUNCH = {"fused_iter": 915_485_952, "pcg": 238_189_568}
 KERNEL_NAMES = {"fused_iter": "k_fused_iter", "pcg": "k_pcg_rows_stream", "line_search": "k_merit_ls",
                 "merit": "k_merit_ls (one step size)"}
 SQP_ITERS, PCG_MAX, PCG_TOL = 5, 173, 1e-5
