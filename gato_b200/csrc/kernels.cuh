@@ -673,14 +673,23 @@ __device__ __forceinline__ void rows_block_sum2(Acc& a, Acc& b, Acc* red)
 struct NoHook {
     __device__ void operator()() const {}
 };
+struct NoDzStage {
+    __device__ bool operator()() const { return false; }
+};
 
 // Sp, Pp: the problem's S and P^-1 (row-major [N n][3n]) in global or shared
 // memory (null: bt.S, bt.P).  hook() runs on every thread after the CG loop,
-// behind a barrier: Sp and Pp are no longer read.
-template <int NQ, typename T, typename Acc, int RPT, class Hook = NoHook>
+// behind a barrier: Sp and Pp are no longer read.  Adz, Qidz: the problem's
+// A_k and Qi_k blocks in shared memory, used by the step recovery on the
+// threads where dz_ready() returns true (each thread decides for itself; no
+// barrier depends on it), else read from global memory.
+template <int NQ, typename T, typename Acc, int RPT, class Hook = NoHook,
+          class DzReady = NoDzStage>
 __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int it_row,
                                               unsigned char* smem_raw, const T* Sp = nullptr,
-                                              const T* Pp = nullptr, Hook hook = Hook())
+                                              const T* Pp = nullptr, Hook hook = Hook(),
+                                              const T* Adz = nullptr, const T* Qidz = nullptr,
+                                              DzReady dz_ready = DzReady())
 {
     constexpr bool HOOK = !std::is_same<Hook, NoHook>::value;
     using RP = RowPcg<NQ, RPT>;
@@ -865,6 +874,9 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
         for (int j = 0; j < RPT; ++j) pv[(k + 1) * VS + i0 + j * TPB] = x[j];
     }
     __syncthreads();
+    const bool dz_st = dz_ready();
+    const T* Ab = dz_st ? Adz : bt.A + (size_t)b * N * n * n;
+    const T* Qib = dz_st ? Qidz : bt.Qi + (size_t)b * N * n * n;
     const T* lk1 = pv + (k + 2) * VS;
     T res[RPT], resu[RPT];
 #pragma unroll
@@ -873,7 +885,7 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
         resu[j] = T(0);
         const int i = i0 + j * TPB;
         if (act) {
-            const T* A = bt.A + ((size_t)b * N + k) * n * n;
+            const T* A = Ab + (size_t)k * n * n;
             T acc = T(0);
             if (k < N - 1) {
 #pragma unroll
@@ -907,7 +919,7 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
 #pragma unroll
         for (int j = 0; j < RPT; ++j) {
             const int i = i0 + j * TPB;
-            const T* Qi = bt.Qi + ((size_t)b * N + k) * n * n;
+            const T* Qi = Qib + (size_t)k * n * n;
             const T* rk = rv + (k + 1) * VS;
             T acc = T(0);
 #pragma unroll
@@ -943,7 +955,10 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
 // next problem and the bulk-copy engine brings its S and P^-1 (2 x 12 N NQ^2
 // floats, contiguous per problem) into shared memory while the CTA computes
 // the step dz, so the matrices load from shared memory instead of as strided
-// rows from HBM.  Claiming at the end rather than the start of a problem
+// rows from HBM.  With dz_stage, a second copy (own mbarrier) brings the
+// problem's A_k and Qi_k blocks when its CG loop starts, for the step
+// recovery after it; each thread waits on it with its own bound and reads
+// global memory if that expires.  Claiming at the end rather than the start of a problem
 // keeps the assignment as adaptive as the hardware's block scheduling (the
 // early claim cost the adjoint's long, uneven CG runs 8 %).  Per-problem arithmetic is that of
 // k_pcg_rows.  Thread 0 alone waits on the copy's mbarrier, with a bound;
@@ -952,6 +967,11 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
 template <int NQ>
 struct PcgStage {
     __host__ __device__ static size_t matrix_floats(int N) { return (size_t)12 * N * NQ * NQ; }
+    __host__ __device__ static size_t block_floats(int N) { return (size_t)4 * N * NQ * NQ; }  // N n x n
+    __host__ __device__ static size_t smem_bytes_dz(int N)
+    {
+        return smem_bytes(N) + 2 * block_floats(N) * sizeof(float);
+    }
     __host__ __device__ static size_t offset(int N)
     {
         return (RowPcg<NQ, 2>::template smem_bytes<float>(N) + 127) & ~(size_t)127;
@@ -966,10 +986,10 @@ constexpr int PCG_STAGE_WAIT_TRIES = 1 << 22;
 
 template <int NQ, typename Acc>
 __global__ void __launch_bounds__(RowPcg<NQ, 2>::MAX_THREADS, 1)
-    k_pcg_rows_stream(Batch<NQ, float> bt, int it_row)
+    k_pcg_rows_stream(Batch<NQ, float> bt, int it_row, int dz_stage)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];  // stage offset 128-aligned
-    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(8) uint64_t bar, bar_dz;
     __shared__ int s_next, s_ok;
     if (*bt.done) return;
     const int N = bt.N, B = bt.B, tid = threadIdx.x;
@@ -977,6 +997,11 @@ __global__ void __launch_bounds__(RowPcg<NQ, 2>::MAX_THREADS, 1)
     float* stS = reinterpret_cast<float*>(smem_raw + PcgStage<NQ>::offset(N));
     float* stP = stS + mat;
     const uint32_t bytes = (uint32_t)(mat * sizeof(float));
+    const size_t blk = PcgStage<NQ>::block_floats(N);
+    float* stA = stP + mat;
+    float* stQi = stA + blk;
+    const uint32_t blk_bytes = (uint32_t)(blk * sizeof(float));
+    uint32_t parity_dz = 0;
     auto fetch = [&](int pb) {  // thread 0; earlier reads of the stage are behind a barrier
         fence_proxy_async_shared();
         mbar_arrive_expect_tx(&bar, 2 * bytes);
@@ -986,6 +1011,7 @@ __global__ void __launch_bounds__(RowPcg<NQ, 2>::MAX_THREADS, 1)
     int b = blockIdx.x;
     if (tid == 0) {
         mbar_init(&bar, 1);
+        mbar_init(&bar_dz, 1);
         fence_mbar_init();
         if (b < B) fetch(b);
     }
@@ -1005,6 +1031,22 @@ __global__ void __launch_bounds__(RowPcg<NQ, 2>::MAX_THREADS, 1)
         }
         if (tid != 0) mbar_try_wait(&bar, parity);  // phase complete: acquires the data
         parity ^= 1;
+        if (dz_stage && tid == 0) {  // the previous problem's dz reads are behind a barrier
+            fence_proxy_async_shared();
+            mbar_arrive_expect_tx(&bar_dz, 2 * blk_bytes);
+            bulk_copy_g2s(stA, bt.A + (size_t)b * blk, blk_bytes, &bar_dz);
+            bulk_copy_g2s(stQi, bt.Qi + (size_t)b * blk, blk_bytes, &bar_dz);
+        }
+        auto dz_ready = [&]() {
+            if (!dz_stage) return false;
+            int i = 0;
+            while (!mbar_try_wait(&bar_dz, parity_dz) && ++i < PCG_STAGE_WAIT_TRIES) {
+            }
+            parity_dz ^= 1;
+            if (i < PCG_STAGE_WAIT_TRIES) return true;
+            atomicExch(bt.work + 2, 1);
+            return false;
+        };
         auto next = [&]() {
             if (tid == 0) {
                 const int nb = (int)gridDim.x + atomicAdd(bt.work, 1);
@@ -1012,7 +1054,8 @@ __global__ void __launch_bounds__(RowPcg<NQ, 2>::MAX_THREADS, 1)
                 if (nb < B) fetch(nb);
             }
         };
-        pcg_rows_body<NQ, float, Acc, 2>(bt, b, it_row, smem_raw, stS, stP, next);
+        pcg_rows_body<NQ, float, Acc, 2>(bt, b, it_row, smem_raw, stS, stP, next, stA, stQi,
+                                         dz_ready);
         __syncthreads();
         b = s_next;
     }

@@ -476,6 +476,17 @@ bool pcg_stream_fits(const gato_solver* s)
         return false;
 }
 
+// ... and the step recovery's A_k, Qi_k blocks too (iiwa14 up to N = 32)
+template <class Tg>
+bool pcg_stream_dz_fits(const gato_solver* s)
+{
+    if constexpr (sizeof(typename Tg::T) == 4)
+        return pcg_stream_fits<Tg>(s) &&
+               PcgStage<Tg::NQ>::smem_bytes_dz(s->N) + 64 <= (size_t)s->max_smem;
+    else
+        return false;
+}
+
 // register-resident PCG + dz of every problem
 template <class Tg>
 void launch_pcg_rows(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt,
@@ -487,8 +498,11 @@ void launch_pcg_rows(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typena
     if constexpr (sizeof(T) == 4) {
         if (pcg_stream_fits<Tg>(s)) {
             const int grid = std::min(s->B, s->nsm);
+            const int dz = pcg_stream_dz_fits<Tg>(s);
             k_pcg_rows_stream<NQ, Acc><<<grid, RowPcg<NQ, 2>::threads(s->N),
-                                         PcgStage<NQ>::smem_bytes(s->N), st>>>(bt, row);
+                                         dz ? PcgStage<NQ>::smem_bytes_dz(s->N)
+                                            : PcgStage<NQ>::smem_bytes(s->N),
+                                         st>>>(bt, row, dz);
             return;
         }
     }
@@ -622,7 +636,10 @@ int configure_kernels(gato_solver* s)
                 s->max_smem));
     if constexpr (sizeof(T) == 4) {
         if (pcg_stream_fits<Tg>(s))
-            RC(set_smem(k_pcg_rows_stream<NQ, Acc>, PcgStage<NQ>::smem_bytes(s->N), s->max_smem));
+            RC(set_smem(k_pcg_rows_stream<NQ, Acc>,
+                        pcg_stream_dz_fits<Tg>(s) ? PcgStage<NQ>::smem_bytes_dz(s->N)
+                                                  : PcgStage<NQ>::smem_bytes(s->N),
+                        s->max_smem));
     }
     return GATO_OK;
 }
