@@ -38,7 +38,7 @@ PLANT, N, DT = "iiwa14", 32, 0.01
 # DRAM bytes (read + write) per launch from one ncu capture of the first SQP
 # iteration of this workload (profiles/k_fused_iter_iiwa14_N32_B1024.md,
 # profiles/k_pcg_rows_stream_iiwa14_N32_B1024.md)
-TRAFFIC_PER_LAUNCH = {"fused_iter": 915_485_952, "pcg": 238_189_568}
+TRAFFIC_PER_LAUNCH = {"fused_iter": 915_485_952, "pcg": 238_636_544}
 KERNEL_NAMES = {"fused_iter": "k_fused_iter", "pcg": "k_pcg_rows_stream", "line_search": "k_merit_ls",
                 "merit": "k_merit_ls (one step size)"}
 SQP_ITERS, PCG_MAX, PCG_TOL = 5, 173, 1e-5
@@ -188,6 +188,9 @@ class ClockSampler:
         os.unlink(self.path)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+HBM_FALLBACK_GBS = 6650.0  # copy bandwidth of this pool's B200s when no measured file is present
 
 
 def measured_peaks():
@@ -658,7 +661,9 @@ def run_ours(args):
                      "kernel": KERNEL_NAMES[top],
                      "peak_source": "measured FP32 SGEMM on this GPU (TF32 off)",
                      "flops_source": "reference device functions run with a counting scalar",
-                     "hbm_peak_gbs": peaks.get("hbm_gbs")},
+                     "hbm_peak_gbs": peaks.get("hbm_gbs", HBM_FALLBACK_GBS),
+                     "hbm_peak_source": "MEASURED_PEAKS.json" if "hbm_gbs" in peaks
+                     else "fallback (earlier measurement on this pool)"},
         "roofline_by_kernel": {KERNEL_NAMES[k]: {kk: round(vv, 4) for kk, vv in v.items()}
                                for k, v in roof.items()},
         "clocks": clk,
