@@ -647,6 +647,8 @@ def run_ours(args):
         "adjoint": {"ms_per_call": ms_adj, "vs_forward_solve": ms_adj / ms_fused,
                     "pcg_iters_mean": {"forward_qp_step": float(adj_its[0].mean()),
                                        "adjoint": float(adj_its[1].mean())},
+                    "pcg_iters_max": {"forward_qp_step": int(adj_its[0].max()),
+                                      "adjoint": int(adj_its[1].max())},
                     "what": "gradients for x0, goals, Q/R diagonals of a dense loss "
                             "gradient (FP32, relative PCG tol 1e-12)"},
         "e2e": {"value": solves / s_e2e, "unit": "solves/s",
