@@ -13,9 +13,15 @@ and L2 is flushed between steps.
   e2e       solves/s through gato_solve_host (host buffers; H2D of XU, x0,
             goals and D2H of XU inside the timed region)
   plain     solves/s of the plain per-kernel form, same workload
-  roofline  FP32 CUDA-core roofline of the dominant kernel (k_fused_iter)
+  by_precision  fused and plain solves/s in FP32, mixed (FP64 reductions)
+            and FP64
+  roofline  FP32 CUDA-core roofline of the kernel with the largest share of
+            device time (the persistent PCG, k_pcg_rows_stream)
   cpu_baseline  the FP64 oracle of the same SQP on the host cores, bounded
             sample of the same workload
+  accuracy_vs_fp64_oracle  every precision's trajectory error against the
+            oracle, the oracle's own FP32-storage floor, and a converged
+            (30-iteration) solve
 
 `--impl reference` times the reference's algorithm on the host CPU (the FP64
 oracle port: the reference's solver has no CPU implementation and its CUDA
@@ -66,28 +72,83 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="problems in the CPU baseline sample (0: sized to ~10 s)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="single", choices=["single", "mixed", "mpc", "sweep"],
+    ap.add_argument("--workload", default="single",
+                    choices=["single", "mixed", "mpc", "sweep", "profile"],
                     help="single: the headline iiwa14 N=32 batch; mixed: 4096 problems of "
-                         "both plants and four horizons in one solve")
+                         "both plants and four horizons in one solve; profile: one solve per "
+                         "form, untimed, as the target of an ncu capture")
+    ap.add_argument("--horizon", type=int, default=N, help="knots (profile workload only)")
+    ap.add_argument("--plant", default=PLANT, help="robot (profile workload only)")
+    ap.add_argument("--sqp-iters", type=int, default=2, help="SQP iterations (profile workload only)")
     return ap.parse_args()
 
 
 # --------------------------------------------------------------------------
+# The workload, built the same way by both arms from the arm's own robot
+# tables and forward kinematics: seeded problems (the formulas of
+# gato_b200/workloads.py: q ~ U(0.8 x limits), qd ~ N(0, 0.1^2), figure-8
+# end-effector goals in the shape of python/bsqp/common.py:27-45), solved in
+# FP64 from the default warm start (30 SQP iterations, PCG tol 1e-6), then
+# perturbed by seeded noise.  Both FP64 solves reproduce each other to about
+# 1e-10, so after rounding to FP32 the two arms start from the same XU and
+# lambda.
+WARM_KW = dict(max_sqp_iters=30, pcg_tol=1e-6, max_pcg_iters=400)
+
+
+def seeded_problems(nq, q_limit, fk, B, seed):
+    """xs [B, 2nq], goal [B, 6N] (float32), the default warm start [B, traj]
+    and the generator state."""
+    rng = np.random.default_rng(seed)
+    lim = np.array([q_limit[i] for i in range(nq)])
+    xs = np.concatenate([rng.uniform(-0.8, 0.8, (B, nq)) * lim, rng.normal(0.0, 0.1, (B, nq))],
+                        axis=1)
+    p0 = fk(xs[:, :nq])
+    centre = p0 + rng.normal(0.0, 0.02, (B, 3))
+    amp, period = rng.uniform(0.1, 0.3, B), rng.uniform(2.0, 6.0, B)
+    phase = rng.uniform(0.0, 2 * np.pi, B)
+    th = np.pi / 4
+    Rz = np.array([[np.cos(th), -np.sin(th), 0.0], [np.sin(th), np.cos(th), 0.0], [0, 0, 1.0]])
+    tau = 2 * np.pi * np.arange(N)[None, :] * DT / period[:, None] + phase[:, None]
+    local = np.stack([amp[:, None] * np.sin(tau), np.zeros_like(tau),
+                      amp[:, None] * np.sin(2 * tau) / 2], axis=-1)
+    goal = np.zeros((B, N, 6))
+    goal[:, :, :3] = centre[:, None, :] + local @ Rz.T
+    nx, nu = 2 * nq, nq
+    xu = np.zeros((B, N, nx + nu))
+    xu[:, :, :nx] = xs[:, None, :]
+    xu = xu.reshape(B, -1)[:, : N * (nx + nu) - nu]
+    return (xs.astype(np.float32), goal.reshape(B, 6 * N).astype(np.float32),
+            xu.astype(np.float32), rng)
+
+
+def perturbed_warm_start(xu_conv, lam, xs, nq, rng):
+    """q, qd + N(0, 0.01^2) and u + N(0, 0.1^2) on every knot but x_0."""
+    B = xu_conv.shape[0]
+    nx, nu = 2 * nq, nq
+    full = np.zeros((B, N * (nx + nu)))
+    full[:, : xu_conv.shape[1]] = xu_conv
+    full = full.reshape(B, N, nx + nu)
+    full[:, 1:, :nx] += rng.normal(0.0, 0.01, (B, N - 1, nx))
+    full[:, :, nx:] += rng.normal(0.0, 0.1, (B, N, nu))
+    xu0 = full.reshape(B, -1)[:, : xu_conv.shape[1]].astype(np.float32)
+    xu0[:, :nx] = xs
+    return dict(xs=xs, xu=xu0, lam=np.asarray(lam).astype(np.float32))
+
+
 def make_workload(batch, seed):
-    """Synthetic inputs plus a warm start: the fused solver run to
-    convergence from the default warm start, perturbed by seeded noise."""
+    """This arm's copy: the library's robot tables and kinematics, warm
+    start from its FP64 solver."""
     import gato_b200
-    from gato_b200 import workloads as W
-    pr = W.make_problem(PLANT, N, batch, seed=seed, goals="figure8", dt=DT)
-    kw = solver_kwargs()
-    kw.update(max_sqp_iters=30, pcg_tol=1e-6, max_pcg_iters=400)
-    s = gato_b200.BSQP(batch_size=batch, N=N, dt=DT, plant_type=PLANT, form="fused", **kw)
-    res = s.solve_raw(pr["xu"], DT, pr["xs"], pr["goal"])
+    from gato_b200.kinematics import ee_position
+    model = gato_b200.builtin_model(PLANT)
+    xs, goal, xu, rng = seeded_problems(model.nq, model.q_limit,
+                                        lambda q: ee_position(model, q), batch, seed)
+    s = gato_b200.BSQP(batch_size=batch, N=N, dt=DT, plant_type=PLANT, form="fused",
+                       precision="fp64", **dict(solver_kwargs(), **WARM_KW))
+    res = s.solve_raw(xu.astype(np.float64), DT, xs.astype(np.float64), goal.astype(np.float64))
     lam = s.get_lambda()
     s.close()
-    xu0 = W.perturb(res["XU"], 7, N, pr["rng"]).astype(np.float32)
-    xu0[:, :14] = pr["xs"]
-    return dict(xs=pr["xs"], goal=pr["goal"], xu=xu0, lam=lam)
+    return dict(perturbed_warm_start(res["XU"], lam, xs, model.nq, rng), goal=goal)
 
 
 # Per-knot FLOPs of the reference's own device functions for iiwa14, counted
@@ -190,7 +251,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-HBM_FALLBACK_GBS = 6650.0  # copy bandwidth of this pool's B200s when no measured file is present
+HBM_FALLBACK_GBS = 6650.0  # B200 copy bandwidth measured earlier, used when no measured-peaks file is present
 
 
 def measured_peaks():
@@ -275,7 +336,7 @@ def run_reference(args):
         return 0
     threads = os.cpu_count() or 1
     sample = args.cpu_sample or max(threads, min(args.batch, 8 * threads))
-    wl = make_cpu_workload(args.batch, sample, threads)
+    wl = make_reference_workload(args.batch, replica_seed(0), threads)
     for _ in range(args.warmup):
         cpu_baseline(wl, min(sample, threads), threads)
     times = []
@@ -283,14 +344,16 @@ def run_reference(args):
         v, dt = cpu_baseline(wl, sample, threads)
         times.append(dt)
     value = args.steps * sample / float(np.sum(times))
-    ref_gpu = reference_gpu_leg(args)
+    ref_gpu = reference_gpu_leg(args, wl)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "global_batch": args.batch, "seq_len": N,
-                   "parallelism": f"{threads} host threads"},
+                   "parallelism": f"{threads} host threads",
+                   "warm_start": "FP64 oracle, 30 SQP iterations, then the seeded perturbation "
+                                 "(the same XU and lambda as the other arm to FP32 rounding)"},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
                          "sample": f"{sample} problems of the workload per step (FP64 oracle "
                                    f"port of the reference SQP; the reference's solver has "
@@ -306,12 +369,15 @@ def run_reference(args):
 _REF_MODULE = {}
 
 
-def reference_gpu_leg(args, B=None):
+def reference_gpu_leg(args, wl):
     """The reference's own CUDA solver (python/bindings.cu compiled unmodified
     for sm_100a into oracle/_ref by oracle/build_ref_gpu.py) on the same
-    workload, through its own solve(): host arrays in, host arrays out, as
-    its Python interface calls it.  Reported beside the CPU arm; absent
-    module or GPU gives an "unavailable" entry."""
+    workload `wl` (make_reference_workload), through its own solve(): host
+    arrays in, host arrays out, as its Python interface calls it.  Reported
+    beside the CPU arm; absent module or GPU gives an "unavailable" entry.
+    Its lambda lives inside the module with no setter: it starts at zero and
+    carries from call to call, the one input that differs from the other
+    arm."""
     import glob
     import importlib.util
     paths = glob.glob(os.path.join(ROOT, "oracle", "_ref", f"bsqpN{N}_{PLANT}*.so"))
@@ -331,36 +397,21 @@ def reference_gpu_leg(args, B=None):
         spec.loader.exec_module(mod)
         _REF_MODULE[name] = mod
     mod = _REF_MODULE[name]
-    B = B or args.batch
+    B = wl["xu"].shape[0]
     cls = getattr(mod, f"BSQP_{B}_float", None)
     if cls is None:
         return {"unavailable": f"the reference module has no batch-{B} class"}
-    from gato_b200 import workloads as W
-
-    def make(kw):
-        return cls(DT, kw["max_sqp_iters"], kw["kkt_tol"], kw["max_pcg_iters"], kw["pcg_tol"],
-                   kw["solve_ratio"], kw["mu"], kw["q_cost"], kw["qd_cost"], kw["u_cost"],
-                   kw["N_cost"], kw["q_lim_cost"], kw["vel_lim_cost"], kw["ctrl_lim_cost"],
-                   kw["rho"])
-
-    # warm start made as for the other arms: the seeded problems solved to
-    # convergence from the default warm start (here by the reference itself),
-    # then the same seeded perturbation
-    pr = W.make_problem(PLANT, N, B, seed=2026, goals="figure8", dt=DT)
     kw = solver_kwargs()
-    kw30 = dict(kw, max_sqp_iters=30, pcg_tol=1e-6, max_pcg_iters=400)
-    conv = make(kw30)
+    solver = cls(DT, kw["max_sqp_iters"], kw["kkt_tol"], kw["max_pcg_iters"], kw["pcg_tol"],
+                 kw["solve_ratio"], kw["mu"], kw["q_cost"], kw["qd_cost"], kw["u_cost"],
+                 kw["N_cost"], kw["q_lim_cost"], kw["vel_lim_cost"], kw["ctrl_lim_cost"],
+                 kw["rho"])
     f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)
-    res = conv.solve(f32(pr["xu"]), DT, f32(pr["xs"]), f32(pr["goal"]))
-    del conv
-    xu0 = W.perturb(np.array(res["XU"]), 7, N, pr["rng"]).astype(np.float32)
-    xu0[:, :14] = pr["xs"]
-    xs, goal = f32(pr["xs"]), f32(pr["goal"])
-    solver = make(kw)
+    xs, goal = f32(wl["xs"]), f32(wl["goal"])
     wall, own = [], []
     for i in range(args.warmup + args.steps):
         solver.reset_rho()
-        xin = xu0.copy()
+        xin = f32(wl["xu"]).copy()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         out = solver.solve(xin, DT, xs, goal)
@@ -374,32 +425,25 @@ def reference_gpu_leg(args, B=None):
             "ms_per_step": 1e3 * float(np.mean(wall)),
             "p50_ms": 1e3 * float(np.median(wall)), "p99_ms": 1e3 * float(np.percentile(wall, 99)),
             "kind": "reference CUDA build, FP32 -use_fast_math, sm_100a",
-            "note": "solve() with host arrays (its own H2D/D2H inside); lambda carried "
-                    "between calls as the reference keeps it; rho reset before each call",
+            "note": "solve() with host arrays (its own H2D/D2H inside); the same XU warm "
+                    "start as the other arm; lambda internal to the module (zero at the "
+                    "first call, then carried between calls); rho reset before each call",
             "pcg_iters_mean": float(pcg.mean()) if pcg.size else None}
 
 
-def make_cpu_workload(batch, sample, threads):
-    """The reference arm's copy of the workload: the same seeded problems
-    (first `sample` of the batch) with the warm start made the same way, by
-    a 30-iteration solve from the default warm start (here in the FP64 CPU
-    implementation) and the same seeded perturbation."""
-    from gato_b200 import workloads as W
+def make_reference_workload(batch, seed, threads):
+    """The reference arm's copy of the workload: the oracle's robot tables and
+    forward kinematics, warm start from the FP64 oracle.  Nothing of this
+    library is imported on this arm."""
     from oracle import oracle as O
-    pr = W.make_problem(PLANT, N, batch, seed=2026, goals="figure8", dt=DT)
-    kw = solver_kwargs()
-    kw.update(max_sqp_iters=30, pcg_tol=1e-6, max_pcg_iters=400)
-    S = O.Solver(PLANT, N, sample, O.make_params(dt=DT, **kw), threads=threads)
-    xu, _ = S.solve(pr["xu"][:sample].astype(np.float64), DT, pr["xs"][:sample],
-                    pr["goal"][:sample])
-    lam = S.get_lambda()
-    full = np.zeros((batch, xu.shape[1]), np.float32)
-    full[:sample] = xu
-    xu0 = W.perturb(full, 7, N, pr["rng"]).astype(np.float32)
-    xu0[:, :14] = pr["xs"]
-    lam_full = np.zeros((batch, lam.shape[1]), np.float32)
-    lam_full[:sample] = lam
-    return dict(xs=pr["xs"], goal=pr["goal"], xu=xu0, lam=lam_full)
+    model = O.builtin_model(PLANT)
+    m = O.Model(PLANT)
+    fk = lambda q: np.stack([m.ee_pos(qq) for qq in np.asarray(q, np.float64)])
+    xs, goal, xu, rng = seeded_problems(model.nq, model.q_limit, fk, batch, seed)
+    S = O.Solver(PLANT, N, batch, O.make_params(dt=DT, **dict(solver_kwargs(), **WARM_KW)),
+                 threads=threads)
+    xc, _ = S.solve(xu.astype(np.float64), DT, xs.astype(np.float64), goal.astype(np.float64))
+    return dict(perturbed_warm_start(xc, S.get_lambda(), xs, model.nq, rng), goal=goal)
 
 
 # --------------------------------------------------------------------------
@@ -441,13 +485,129 @@ def time_device_steps(torch, solver, bufs, wl, steps, warmup, flush, stream):
         e1 = torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
             e0.record(stream)
-            L.check(L.load().gato_solve(solver._h, stream.cuda_stream, L.vptr(d_xu),
-                                        L.vptr(d_xs), L.vptr(d_goal), None))
+            fn = L.load().gato_solve_f64 if solver.precision == "fp64" else L.load().gato_solve
+            L.check(fn(solver._h, stream.cuda_stream, L.vptr(d_xu), L.vptr(d_xs),
+                       L.vptr(d_goal), None))
             e1.record(stream)
         torch.cuda.synchronize()
         if i >= warmup:
             times.append(e0.elapsed_time(e1))
     return np.array(times)
+
+
+PRECISIONS = ("fp32", "mixed", "fp64")
+
+
+def precision_times(torch, dev, B, prec, wl, args, flush, stream):
+    """Mean ms per solve of the fused and the plain form in precision
+    `prec` on the workload (inputs resident, timed like the headline)."""
+    import gato_b200
+    dt = torch.float64 if prec == "fp64" else torch.float32
+    T = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
+    d_xu0, d_xs, d_goal = T(wl["xu"]), T(wl["xs"]), T(wl["goal"])
+    bufs = (d_xu0.clone(), d_xs, d_goal, d_xu0)
+    out = []
+    for form in ("fused", "plain"):
+        s = gato_b200.BSQP(batch_size=B, N=N, dt=DT, plant_type=PLANT, form=form,
+                           precision=prec, **solver_kwargs())
+        steps = args.steps if form == "fused" else max(3, args.steps // 2)
+        out.append(float(np.mean(time_device_steps(torch, s, bufs, wl, steps, max(1, args.warmup),
+                                                   flush, stream))))
+        s.close()
+    return out
+
+
+def trajectory_errors(xg, xo):
+    """Per problem max |XU - XU_oracle| / max(1, max |XU_oracle|)."""
+    return np.abs(xg - xo).max(axis=1) / np.maximum(1.0, np.abs(xo).max(axis=1))
+
+
+def compare_with_oracle(xg, pcg_g, step_g, xo, pcg_o, step_o):
+    """Trajectory error statistics, PCG-count agreement and the problems
+    whose line-search decision differs from the oracle's, each with the
+    first SQP iteration at which it differs."""
+    e = trajectory_errors(xg, xo)
+    rows = min(step_g.shape[0], step_o.shape[0])
+    diff = step_g[:rows] != np.asarray(step_o[:rows], np.float32)
+    div = np.nonzero(diff.any(axis=0))[0]
+    agree = np.ones(e.shape[0], bool)
+    agree[div] = False
+    out = {"xu_rel_err_median": float(np.median(e)), "xu_rel_err_p90": float(np.percentile(e, 90)),
+           "xu_rel_err_max": float(e.max()), "frac_within_1e-4": float(np.mean(e <= 1e-4)),
+           "pcg_iters_equal_frac": float(np.mean(pcg_g[:rows] == pcg_o[:rows])),
+           "ls_diverged_problems": int(div.size),
+           "ls_first_divergent_iteration": {int(b): int(diff[:, b].argmax()) for b in div},
+           "xu_rel_err_median_where_ls_agrees": float(np.median(e[agree])) if agree.any()
+           else None}
+    return out
+
+
+def accuracy_block(wl, sample, threads, xo, so):
+    """Each precision's fused solve of the first `sample` problems against
+    the FP64 oracle of the same SQP from the same XU, lambda and rho:
+      per precision   trajectory error, PCG counts, line-search divergences
+      fp32_storage_floor  the oracle itself with every stored stage output
+                      (KKT blocks, Schur system, lambda, XU) rounded to FP32
+                      and all arithmetic in FP64: the error an ideal FP32
+                      solver would show
+      converged       30 SQP iterations at PCG tol 1e-6 (sample of 256):
+                      trajectory error and the dynamics defect / KKT
+                      stationarity (FP64 KKT blocks) of each result beside
+                      the oracle's"""
+    import gato_b200
+    from oracle import oracle as O
+    out = {"sample": sample}
+    xs, goal = wl["xs"][:sample], wl["goal"][:sample]
+
+    def gpu(prec, kwx=None, n=sample):
+        s = gato_b200.BSQP(batch_size=n, N=N, dt=DT, plant_type=PLANT, form="fused",
+                           precision=prec, **dict(solver_kwargs(), **(kwx or {})))
+        f = np.float64 if prec == "fp64" else np.float32
+        s.set_lambda(wl["lam"][:n].astype(f))
+        s.reset_rho()
+        g = s.solve_raw(wl["xu"][:n].astype(f), DT, xs[:n].astype(f), goal[:n].astype(f))
+        lam = s.get_lambda().astype(np.float64)
+        s.close()
+        return g, lam
+
+    for prec in PRECISIONS:
+        g, _ = gpu(prec)
+        out[prec] = compare_with_oracle(np.asarray(g["XU"], np.float64), g["pcg_iters"],
+                                        g["ls_step_size"], xo, so["pcg_iters"], so["ls_step_size"])
+    S = O.Solver(PLANT, N, sample, O.make_params(dt=DT, **solver_kwargs()), threads=threads)
+    S.set_round_f32(S.ROUND_ALL)
+    S.set_lambda(wl["lam"][:sample].astype(np.float64))
+    xf, sf = S.solve(wl["xu"][:sample].astype(np.float64), DT, xs.astype(np.float64),
+                     goal.astype(np.float64))
+    out["fp32_storage_floor"] = compare_with_oracle(xf, sf["pcg_iters"], sf["ls_step_size"], xo,
+                                                    so["pcg_iters"], so["ls_step_size"])
+    # converged workload
+    kc = min(sample, 256)
+    S = O.Solver(PLANT, N, kc, O.make_params(dt=DT, **dict(solver_kwargs(), **WARM_KW)),
+                 threads=threads)
+    S.set_lambda(wl["lam"][:kc].astype(np.float64))
+    xc, sc = S.solve(wl["xu"][:kc].astype(np.float64), DT, xs[:kc].astype(np.float64),
+                     goal[:kc].astype(np.float64))
+    ks = min(kc, 64)
+    xs64, goal64 = xs[:ks].astype(np.float64), goal[:ks].astype(np.float64)
+    do, so_ = kkt_measures(xc[:ks], S.get_lambda()[:ks], xs64, goal64)
+    conv = {"problems": kc, "sqp_iters": WARM_KW["max_sqp_iters"], "pcg_tol": WARM_KW["pcg_tol"],
+            "oracle": {"defect_median": float(np.median(do)), "stationarity_median":
+                       float(np.median(so_)), "stationarity_max": float(so_.max())}}
+    for prec in PRECISIONS:
+        g, lam = gpu(prec, WARM_KW, kc)
+        xg = np.asarray(g["XU"], np.float64)
+        dg, sg = kkt_measures(xg[:ks], lam[:ks], xs64, goal64)
+        e = trajectory_errors(xg, xc)
+        conv[prec] = {"xu_rel_err_median": float(np.median(e)), "xu_rel_err_max": float(e.max()),
+                      "defect_median": float(np.median(dg)),
+                      "stationarity_median": float(np.median(sg)),
+                      "stationarity_abs_diff_max": float(np.abs(sg - so_).max()),
+                      "defect_abs_diff_max": float(np.abs(dg - do).max())}
+    out["converged"] = conv
+    out["note"] = ("fused solves vs the FP64 oracle of the same SQP, same inputs; defect and "
+                   "stationarity evaluated with FP64 KKT blocks at each solver's own result")
+    return out
 
 
 def run_ours(args):
@@ -565,6 +725,19 @@ def run_ours(args):
     p50 = max_over_ranks(float(np.median(t_fused)), dist, dev)
     p99 = max_over_ranks(float(np.percentile(t_fused, 99)), dist, dev)
 
+    # the other precisions' throughput on the same workload (fused and plain)
+    by_prec = {args.precision: {"value": B / (float(np.mean(t_fused)) * 1e-3),
+                                "plain_value": B / (float(np.mean(t_plain)) * 1e-3),
+                                "fused_vs_plain": float(np.mean(t_plain) / np.mean(t_fused))}}
+    for prec in PRECISIONS:
+        if prec in by_prec:
+            continue
+        tf, tp = precision_times(torch, dev, B, prec, wl, args, flush, stream)
+        by_prec[prec] = {"value": B / (tf * 1e-3), "plain_value": B / (tp * 1e-3),
+                         "fused_vs_plain": tp / tf}
+    by_prec = {k: {kk: max_over_ranks(vv, dist, dev) for kk, vv in v.items()}
+               for k, v in by_prec.items()}
+
     # CPU baseline (rank 0, N=1 only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -574,38 +747,7 @@ def run_ours(args):
         cpu = {"value": v, "unit": "solves/s", "cores": threads, "kind": "port",
                "sample": f"{sample} problems of the workload, one solve, {secs:.1f} s wall "
                          f"(FP64 oracle port of the reference SQP)"}
-        # the oracle as the checker: the FP32 solution of the same problems
-        # from the same warm start, lambda and rho
-        d_xu.copy_(d_xu0)
-        fused.set_lambda(wl["lam"])
-        fused.reset_rho()
-        stg = fused.solve_device(d_xu, d_xs, d_goal, stream=stream.cuda_stream)
-        torch.cuda.synchronize()
-        xg = d_xu.double().cpu().numpy()[:sample]
-        errs = np.abs(xg - xo).max(axis=1) / np.maximum(1.0, np.abs(xo).max(axis=1))
-        ks = min(sample, 64)
-        xs64, goal64 = wl["xs"][:ks].astype(np.float64), wl["goal"][:ks].astype(np.float64)
-        dg, sg = kkt_measures(xg[:ks], fused.get_lambda()[:ks].astype(np.float64), xs64, goal64)
-        do, so_ = kkt_measures(xo[:ks], so["lam"][:ks], xs64, goal64)
-        accuracy = {"sample": sample, "xu_rel_err_max": float(errs.max()),
-                    "xu_rel_err_median": float(np.median(errs)),
-                    "pcg_iters_equal_frac": float(np.mean(
-                        stg["pcg_iters"][:, :sample] == so["pcg_iters"]))
-                    if stg["pcg_iters"].shape[0] == so["pcg_iters"].shape[0] else None,
-                    "dynamics_defect": {"problems": ks, "median": float(np.median(dg)),
-                                        "max": float(dg.max()),
-                                        "oracle_median": float(np.median(do)),
-                                        "oracle_max": float(do.max()),
-                                        "rel_diff_median": float(np.median(
-                                            np.abs(dg - do) / np.maximum(do, 1e-12)))},
-                    "kkt_stationarity": {"problems": ks, "median": float(np.median(sg)),
-                                         "max": float(sg.max()),
-                                         "oracle_median": float(np.median(so_)),
-                                         "oracle_max": float(so_.max()),
-                                         "rel_diff_median": float(np.median(
-                                             np.abs(sg - so_) / np.maximum(so_, 1e-12)))},
-                    "note": "FP32 fused solve vs the FP64 oracle of the same SQP, same inputs; "
-                            "defect and stationarity from FP64 KKT blocks at each result"}
+        accuracy = accuracy_block(wl, sample, threads, xo, so)
     if dist:
         dist.destroy_process_group()
     if rank != 0:
@@ -644,6 +786,7 @@ def run_ours(args):
         "plain_form": {"value": solves / (ms_plain * 1e-3), "unit": "solves/s",
                        "ms_per_step": ms_plain},
         "fused_vs_plain": ms_plain / ms_fused,
+        "by_precision": by_prec,
         "adjoint": {"ms_per_call": ms_adj, "vs_forward_solve": ms_adj / ms_fused,
                     "pcg_iters_mean": {"forward_qp_step": float(adj_its[0].mean()),
                                        "adjoint": float(adj_its[1].mean())},
@@ -967,8 +1110,9 @@ def run_sweep(args):
 
 def run_reference_sweep(args):
     rows = []
+    threads = os.cpu_count() or 1
     for B in SWEEP_BATCHES:
-        r = reference_gpu_leg(args, B)
+        r = reference_gpu_leg(args, make_reference_workload(B, 2026, threads))
         r["batch"] = B
         rows.append(r)
     print(json.dumps({"impl": "reference", "metric": "SQP solves/s and latency vs batch size "
@@ -976,8 +1120,44 @@ def run_reference_sweep(args):
     return 0
 
 
+def run_profile(args):
+    """One batched solve in each form, for ncu: a plain-form solve (k_merit,
+    k_merit_sum, then per SQP iteration k_kkt, k_schur_inv, k_schur,
+    k_schur_off, k_pcg, k_dz, k_merit, k_line_search), then a fused-form solve
+    without its CUDA graph (per SQP iteration k_fused_iter or the knot-parallel
+    KKT and Schur kernels, the PCG kernel, k_check, k_merit_ls).  Default
+    warm start perturbed by seeded noise; prints the per-kernel event times."""
+    import ctypes
+    import torch
+    import gato_b200
+    import gato_b200._lib as L
+    from gato_b200 import workloads as W
+    torch.cuda.set_device(0)
+    pr = W.make_problem(args.plant, args.horizon, args.batch, seed=5)
+    nq = pr["model"].nq
+    xu = W.perturb(pr["xu"], nq, args.horizon, pr["rng"]).astype(np.float32)
+    xu[:, :2 * nq] = pr["xs"]
+    kw = dict(max_sqp_iters=args.sqp_iters, pcg_tol=PCG_TOL, max_pcg_iters=PCG_MAX)
+    dev = torch.device("cuda")
+    T = lambda x: torch.tensor(np.ascontiguousarray(x), dtype=torch.float32, device=dev)
+    d_xs, d_goal = T(pr["xs"]), T(pr["goal"])
+    for form in ("plain", "fused"):
+        s = gato_b200.BSQP(batch_size=args.batch, N=args.horizon, dt=DT, plant_type=args.plant,
+                           form=form, precision=args.precision, **kw)
+        d_xu = T(xu)
+        ms = (ctypes.c_double * len(L.KERNELS))()
+        n = (ctypes.c_int32 * len(L.KERNELS))()
+        L.check(L.load().gato_profile_solve(s._h, None, L.vptr(d_xu), L.vptr(d_xs),
+                                            L.vptr(d_goal), ms, n))
+        print(form, {L.KERNELS[i]: round(ms[i], 3) for i in range(len(L.KERNELS)) if n[i]})
+        s.close()
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "profile":
+        return run_profile(args)
     if args.workload == "sweep":
         return run_reference_sweep(args) if args.impl == "reference" else run_sweep(args)
     if args.workload == "mpc":

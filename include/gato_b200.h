@@ -332,7 +332,9 @@ int gato_rollout_backward(gato_solver_t* s, void* stream, int steps,
                           void* d_g_wdiag, double tol, int max_iters);
 
 /* No counterpart in the reference.  The PCG of gato_stage_pcg (FP32 arithmetic
-   and reductions, every problem solved) on caller-owned device buffers, with
+   and reductions, every problem solved), with ONE relative tolerance pcg_tol
+   for all problems (gato_stage_pcg uses the per-problem tolerances of
+   gato_set_pcg_tol_batch), on caller-owned device buffers, with
    no solver handle and no device allocation, for callers that may not
    allocate: a control loop re-solving every millisecond cannot afford
    cudaMalloc's device-wide synchronisation, and some hosts hand all device
@@ -346,7 +348,11 @@ int gato_rollout_backward(gato_solver_t* s, void* stream, int steps,
    calls on one device must not overlap: two calls in flight at once (other
    streams or host threads) race on it.  The first call on each device does
    a one-time set-up (scratch address lookup, kernel attribute) with that
-   device current; make that first call before any stream capture begins. */
+   device current; make that first call before any stream capture begins.
+   The set-up is kept per device for the life of the process: after a
+   cudaDeviceReset of that device (which invalidates the looked-up address
+   and the kernel attribute) do not call this entry point again in the same
+   process. */
 #define GATO_PCG_STATIC_MAX_BATCH 8192
 int gato_pcg_static(void* stream, int nq, int N, int batch, float pcg_tol,
                     int max_pcg_iters, const float* d_S, const float* d_Pinv,

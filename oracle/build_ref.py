@@ -2,7 +2,7 @@
 plant cost and integrator headers compiled for the host in FP64.
 
 Test infrastructure only.  The reference headers are read from where they lie
-(GATO_REF, default /root/reference); the GRiD headers are passed through a
+(reference_root(): $GATO_REF, else the recipe's default location); the GRiD headers are passed through a
 filter that drops their CUDA kernel-launch host wrappers (functions whose body
 contains a `<<<...>>>` launch) and their `__global__` kernels, which g++ cannot
 parse and the oracle does not need.  The filtered tree lives in a temporary
@@ -20,7 +20,19 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF = os.environ.get("GATO_REF", "/root/reference")
+# The only place the reference tree's location is written: this recipe reads
+# the reference's sources where they lie.  $GATO_REF overrides it.
+DEFAULT_REF = "/root/reference"
+
+
+def reference_root():
+    """The reference source tree ($GATO_REF, else DEFAULT_REF), or None when
+    neither holds it (nothing of oracle/_ref can be built then)."""
+    root = os.environ.get("GATO_REF") or DEFAULT_REF
+    return root if os.path.isdir(os.path.join(root, "gato")) else None
+
+
+REF = reference_root() or (os.environ.get("GATO_REF") or DEFAULT_REF)
 
 HEADERS = [
     "settings.h",

@@ -6,7 +6,7 @@ the flags of the reference's CMakeLists.txt release build: -O3
 
 This is a measurement baseline, not the oracle: it is FP32 with fast math.
 nvcc is run directly on the reference's python/bindings.cu where it lies
-(GATO_REF, default /root/reference); nothing is copied.  One module takes
+(build_ref.reference_root()); nothing is copied.  One module takes
 several minutes to compile.
 
 Only the FP32 build is made: the reference's USE_DOUBLES build raised an
@@ -21,7 +21,10 @@ import sysconfig
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF = os.environ.get("GATO_REF", "/root/reference")
+sys.path.insert(0, HERE)
+from build_ref import reference_root  # noqa: E402
+
+REF = reference_root()
 
 
 def module_path(plant, N):
@@ -30,6 +33,8 @@ def module_path(plant, N):
 
 def build(plant, N, force=False):
     out = module_path(plant, N)
+    if REF is None:
+        raise FileNotFoundError("reference tree not found: set GATO_REF to its location")
     src = os.path.join(REF, "python", "bindings.cu")
     if not os.path.exists(src):
         raise FileNotFoundError(f"reference source {src} not present")

@@ -75,7 +75,10 @@ def make_params(**kw):
 def build():
     """Compiles liboracle.so (and oracle/_ref when the reference tree exists)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if os.path.isdir(os.environ.get("GATO_REF", "/root/reference") + "/gato"):
+    import sys
+    sys.path.insert(0, HERE)
+    from build_ref import reference_root
+    if reference_root():
         subprocess.run(["python", os.path.join(HERE, "build_ref.py")], check=True,
                        stdout=subprocess.DEVNULL)
 
@@ -123,6 +126,7 @@ def _load():
         "orc_solver_set_fext": (None, [vp, _dp]),
         "orc_solver_set_cost_diag": (None, [vp, _dp]),
         "orc_solver_set_adapt": (None, [vp, ctypes.c_int]),
+        "orc_solver_set_round_f32": (None, [vp, ctypes.c_int]),
         "orc_solver_reset_dual": (None, [vp]),
         "orc_solver_reset_rho": (None, [vp]),
         "orc_solver_get_lambda": (None, [vp, _dp]),
@@ -331,6 +335,16 @@ class Solver:
 
     def set_rho_adaptation(self, on):
         lib().orc_solver_set_adapt(self.h, int(bool(on)))
+
+    # orc_solver_set_round_f32 flags
+    ROUND_KKT, ROUND_SCHUR, ROUND_LAMBDA, ROUND_XU = 1, 2, 4, 8
+    ROUND_ALL = 15
+
+    def set_round_f32(self, flags):
+        """Rounds the stored stage outputs named by `flags` to FP32 with all
+        arithmetic in FP64: the accuracy floor of an ideal FP32 solver
+        (0 restores exact FP64)."""
+        lib().orc_solver_set_round_f32(self.h, int(flags))
 
     def reset_dual(self):
         lib().orc_solver_reset_dual(self.h)

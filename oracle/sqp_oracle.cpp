@@ -1043,7 +1043,26 @@ struct Solver {
     std::vector<double> wdiag;  // [Bn][nx+nu] when set
     std::vector<double> rho_init, drho_init;
     int threads = 1;
+    /* ORC_ROUND_* flags: stage outputs rounded to FP32 where they are stored
+       (orc_solver_set_round_f32) */
+    int round_f32 = 0;
 };
+
+/* Rounding of stored stage outputs to FP32, with every operation in FP64:
+   the arithmetic of an ideal FP32 solver (each stored value the nearest
+   float to the exact one).  Measures the accuracy floor of any solver that
+   keeps these arrays in FP32; it is not a model of the reference's
+   rounding. */
+enum {
+    ORC_ROUND_KKT = 1,    /* Q, R, q, r, A, B, c after the KKT set-up */
+    ORC_ROUND_SCHUR = 2,  /* S, P^-1, gamma, (Q+rho I)^-1, R^-1 */
+    ORC_ROUND_LAMBDA = 4, /* lambda after the PCG */
+    ORC_ROUND_XU = 8      /* XU after the line-search update */
+};
+static void round_f32(double* p, size_t n)
+{
+    for (size_t i = 0; i < n; ++i) p[i] = (double)(float)p[i];
+}
 
 struct SolveOut {
     int ls_num_iters;
@@ -1089,11 +1108,28 @@ static void solve(Solver& S, double dt, double* xu, const double* xs, const doub
             double* cb = &c[b * N * nx];
             setup_kkt(m, Pb[b], d, dt, xu + b * T, xs + b * nx, goal + b * 6 * N, fext_of(b), Qb,
                       Rb, qb, rb, Ab, Bb, cb);
+            if (S.round_f32 & ORC_ROUND_KKT) {
+                round_f32(Qb, (size_t)N * nx * nx);
+                round_f32(Rb, (size_t)N * nu * nu);
+                round_f32(qb, (size_t)N * nx);
+                round_f32(rb, (size_t)N * nu);
+                round_f32(Ab, (size_t)N * nx * nx);
+                round_f32(Bb, (size_t)N * nx * nu);
+                round_f32(cb, (size_t)N * nx);
+            }
             form_schur(d, S.rho[b], Qb, Rb, qb, rb, Ab, Bb, cb, &Sm[b * d.b3d()],
                        &Pi[b * d.b3d()], &gam[b * L]);
+            if (S.round_f32 & ORC_ROUND_SCHUR) {
+                round_f32(&Sm[b * d.b3d()], d.b3d());
+                round_f32(&Pi[b * d.b3d()], d.b3d());
+                round_f32(&gam[b * L], L);
+                round_f32(Qb, (size_t)N * nx * nx);
+                round_f32(Rb, (size_t)N * nu * nu);
+            }
             pcg_it[b] = conv[b] ? 0
                                 : pcg(d, &Sm[b * d.b3d()], &Pi[b * d.b3d()], &gam[b * L],
                                       &S.lambda[b * L], S.tol[b], P.max_pcg_iters);
+            if (S.round_f32 & ORC_ROUND_LAMBDA) round_f32(&S.lambda[b * L], L);
             compute_dz(d, &S.lambda[b * L], Qb, Rb, qb, rb, Ab, Bb, &dz[b * T]);
         });
         out.pcg_iters.insert(out.pcg_iters.end(), pcg_it.begin(), pcg_it.end());
@@ -1136,6 +1172,7 @@ static void solve(Solver& S, double dt, double* xu, const double* xs, const doub
                 merit_init[b] = best;
                 step[b] = a;
                 for (int i = 0; i < T; ++i) xb[i] += a * dz[b * T + i];
+                if (S.round_f32 & ORC_ROUND_XU) round_f32(xb, T);
             }
         });
         out.ls_num_iters++;
@@ -1328,6 +1365,8 @@ void orc_solver_set_cost_diag(void* h, const double* v)
         S->wdiag.clear();
 }
 void orc_solver_set_adapt(void* h, int on) { ((Solver*)h)->adapt_rho = on != 0; }
+/* flags: ORC_ROUND_* (0 = exact FP64 throughout, the default) */
+void orc_solver_set_round_f32(void* h, int flags) { ((Solver*)h)->round_f32 = flags; }
 void orc_solver_reset_dual(void* h)
 {
     Solver* S = (Solver*)h;

@@ -75,3 +75,32 @@ def test_reference_build_matches_fixtures_when_present(oracle_mod):
         qdd, df = ref.fd_grad(g["q"][0], g["qd"][0], g["u"][0])
         if not g["has_fext"][0]:
             np.testing.assert_array_equal(qdd, g["qdd"][0])
+
+
+def test_fp32_storage_floor_option(oracle_mod):
+    """orc_solver_set_round_f32: with no flags the solve is the exact FP64
+    solve, bit for bit; with every flag the stored stage outputs are FP32
+    values and the result moves by a small, nonzero amount.  The Schur
+    system's rounding dominates the floor (XU rounding alone moves far
+    less)."""
+    O = oracle_mod
+    from gato_b200 import workloads as W
+    N, B = 32, 8
+    pr = W.make_problem("iiwa14", N, B, seed=19)
+    xu = W.perturb(pr["xu"], 7, N, pr["rng"]).astype(np.float64)
+    xu[:, :14] = pr["xs"]
+    P = O.make_params(dt=0.01, max_sqp_iters=5, pcg_tol=1e-5, max_pcg_iters=173)
+    outs = {}
+    for name, flags in (("exact", None), ("zero", 0), ("all", O.Solver.ROUND_ALL),
+                        ("xu", O.Solver.ROUND_XU)):
+        S = O.Solver("iiwa14", N, B, P, threads=2)
+        if flags is not None:
+            S.set_round_f32(flags)
+        outs[name] = S.solve(xu, 0.01, pr["xs"], pr["goal"])[0]
+    np.testing.assert_array_equal(outs["exact"], outs["zero"])
+    err = lambda a: np.abs(a - outs["exact"]).max(1) / np.maximum(1, np.abs(outs["exact"]).max(1))
+    e_all, e_xu = err(outs["all"]), err(outs["xu"])
+    assert np.all(e_all > 0) and np.median(e_all) < 1e-2, e_all
+    assert np.median(e_xu) < np.median(e_all), (e_xu, e_all)
+    # every XU value of the all-rounded solve is a float32 value
+    np.testing.assert_array_equal(outs["all"], outs["all"].astype(np.float32).astype(np.float64))
