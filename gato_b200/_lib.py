@@ -13,6 +13,8 @@ GATO_MAX_NQ = 8
 PLANTS = {"iiwa14": 0, "indy7": 1}
 FORMS = {"plain": 0, "fused": 1}
 PRECISIONS = {"fp32": 0, "mixed": 1, "fp64": 2}
+# per-problem status bits (GATO_STATUS_*)
+STATUS = {"converged": 1, "max_iter": 2, "ls_fail": 4, "nonfinite": 8, "pcg_max_iter": 16}
 KERNELS = ["kkt", "schur", "pcg", "dz", "merit", "line_search", "fused_iter", "check",
            "merit_sum"]
 
@@ -76,6 +78,7 @@ class GatoStats(ctypes.Structure):
         ("pcg_iters", _ip),
         ("ls_min_merit", _fp),
         ("ls_step_size", _fp),
+        ("status", _ip),
     ]
 
 
@@ -101,6 +104,7 @@ SIGNATURES = {
     "gato_set_mu_batch": (ctypes.c_int, [_vp, _fp]),
     "gato_set_pcg_tol_batch": (ctypes.c_int, [_vp, _fp]),
     "gato_set_dt": (ctypes.c_int, [_vp, ctypes.c_float]),
+    "gato_set_wait_limits": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     "gato_reset_dual": (ctypes.c_int, [_vp]),
     "gato_reset_rho": (ctypes.c_int, [_vp]),
     "gato_set_rho_adaptation": (ctypes.c_int, [_vp, ctypes.c_int]),

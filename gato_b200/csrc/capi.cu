@@ -98,6 +98,7 @@ int gato_create(const gato_model_t* model, int N, int batch, const gato_params_t
     RC(p->alloc(&p->done, 1));
     RC(p->alloc(&p->work, 4));
     RC(p->alloc(&p->ls_count, 1));
+    RC(p->alloc(&p->status, B));
     RC(p->alloc(&p->h_pcg, (size_t)iters * B));
     RC(p->alloc(&p->h_ls_min, (size_t)iters * B));
     RC(p->alloc(&p->h_ls_step, (size_t)iters * B));
@@ -208,12 +209,13 @@ int gato_profile_solve(gato_solver_t* s, void* stream, float* d_xu, const float*
     cudaStream_t st = as_stream(stream);
     std::vector<gato_solver::ProfEntry> entries;
     s->prof = &entries;
-    std::vector<int> hs(s->B), hc(s->B);
+    std::vector<int> hs(s->B), hc(s->B), hst(s->B);
     int rows = 0;
     int rc = dispatch(s, [&](auto tg) {
         using Tg = decltype(tg);
         if (s->form == GATO_FORM_PLAIN)
-            return solve_plain<Tg>(s, st, d_xu, d_xs, d_goal, hs.data(), hc.data(), &rows);
+            return solve_plain<Tg>(s, st, d_xu, d_xs, d_goal, hs.data(), hc.data(), hst.data(),
+                                   &rows);
         return enqueue_fused<Tg>(s, st, d_xu, d_xs, d_goal);
     });
     s->prof = nullptr;
@@ -234,6 +236,15 @@ int gato_profile_solve(gato_solver_t* s, void* stream, float* d_xu, const float*
     if (rc) return rc;
     if (e != cudaSuccess) return fail(GATO_ERR_CUDA, "profile solve: %s", cudaGetErrorString(e));
     return check_device_waits(s);
+}
+
+int gato_set_wait_limits(gato_solver_t* s, int copy_tries, int step_copy_tries)
+{
+    RC(check_handle(s));
+    s->wait_tries = copy_tries < 0 ? PCG_STAGE_WAIT_TRIES : copy_tries;
+    s->wait_tries_dz = step_copy_tries < 0 ? PCG_STAGE_WAIT_TRIES : step_copy_tries;
+    s->version++;  // kernel arguments of the cached graph change
+    return GATO_OK;
 }
 
 int gato_set_f_ext_batch(gato_solver_t* s, const float* h_f_ext)

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/gato_b200.h"  // status bits shared with the host
+
 namespace gato {
 
 constexpr int WARP = 32;
@@ -151,6 +153,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
         : "r"(smem_addr(bar)), "r"(parity), "r"(1000u)
         : "memory");
     return ok != 0;
+}
+// true once the phase completes, with at most `tries` try_wait calls (0: gives
+// up at once without looking)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int tries)
+{
+    for (int i = 0; i < tries; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
 }
 
 }  // namespace gato

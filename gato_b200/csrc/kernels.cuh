@@ -45,6 +45,10 @@ struct Batch {
     // bounded wait expired (both counters are back at 0 after each launch)
     int* work;
     int* ls_count;         // line-search iterations run (fused form)
+    int* status;           // [B] GATO_STATUS_* bits found on the device
+    // bounds (mbarrier try_wait calls) of the persistent PCG's waits for its
+    // bulk copies: S and P^-1, and the step recovery's A_k, Qi_k
+    int wait_tries, wait_tries_dz;
     // per-iteration statistics [iter][B]
     int* h_pcg;
     float *h_ls_min, *h_ls_step;
@@ -74,9 +78,11 @@ __global__ void k_merit(Batch<NQ, T> bt, DevModel<NQ, T> M, int nalpha, int use_
     if (lane_id() == 0) bt.merit_terms[((size_t)b * NUM_ALPHAS + j) * N + k] = (double)v;
 }
 
-// Sum of the alpha = 1 terms into out[b] (initial / final merit).
+// Sum of the alpha = 1 terms into out[b] (initial / final merit); a
+// non-finite merit marks the problem's status.
 template <typename Acc>
-__global__ void k_merit_sum(int B, int N, const double* terms, double* out, double* out2)
+__global__ void k_merit_sum(int B, int N, const double* terms, double* out, double* out2,
+                            int* status)
 {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= B) return;
@@ -84,6 +90,19 @@ __global__ void k_merit_sum(int B, int N, const double* terms, double* out, doub
     for (int k = 0; k < N; ++k) s += (Acc)terms[(size_t)b * NUM_ALPHAS * N + k];
     out[b] = (double)s;
     if (out2) out2[b] = (double)s;
+    if (!isfinite((double)s)) status[b] |= GATO_STATUS_NONFINITE;
+}
+
+// Status bits of one line search: no trial step lowered the merit, and
+// every trial merit non-finite (the step itself is not finite).
+template <typename Acc>
+__device__ __forceinline__ int ls_status(const Acc* s_m, bool ok)
+{
+    int st = ok ? 0 : GATO_STATUS_LS_FAIL;
+    bool any = false;
+    for (int j = 0; j < NUM_ALPHAS; ++j) any |= isfinite((double)s_m[j]);
+    if (!any) st |= GATO_STATUS_NONFINITE;
+    return st;
 }
 
 // ------------------------------------------------------------------ line search
@@ -117,6 +136,7 @@ __global__ void k_line_search(Batch<NQ, T> bt, int it, int skip_if_done)
             }
         const Acc m0 = (Acc)bt.merit_init[b];
         const bool ok = best < m0;
+        bt.status[b] |= ls_status<Acc>(s_m, ok);
         if (bt.adapt_rho) {
             const T dr = bt.drho[b];
             const T fac = T(RHO_FACTOR);
@@ -191,6 +211,7 @@ __device__ __forceinline__ void merit_ls_body(const Batch<NQ, T>& bt, const DevM
     __syncthreads();
     if (mode != 1) {
         if (t == 0) {
+            if (!isfinite((double)s_m[0])) bt.status[b] |= GATO_STATUS_NONFINITE;
             if (mode == 0) {
                 bt.merit_init[b] = (double)s_m[0];
                 bt.merit_init0[b] = (double)s_m[0];
@@ -209,6 +230,7 @@ __device__ __forceinline__ void merit_ls_body(const Batch<NQ, T>& bt, const DevM
                 bj = j;
             }
         const bool ok = best < (Acc)bt.merit_init[b];
+        bt.status[b] |= ls_status<Acc>(s_m, ok);
         if (bt.adapt_rho) {
             const T dr = bt.drho[b];
             const T fac = T(RHO_FACTOR);
@@ -961,9 +983,18 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
 // global memory if that expires.  Claiming at the end rather than the start of a problem
 // keeps the assignment as adaptive as the hardware's block scheduling (the
 // early claim cost the adjoint's long, uneven CG runs 8 %).  Per-problem arithmetic is that of
-// k_pcg_rows.  Thread 0 alone waits on the copy's mbarrier, with a bound;
-// the outcome goes through shared memory so that every thread takes the same
-// branch.  An expired wait sets bt.work[2] and ends the CTA.
+// k_pcg_rows.  Thread 0 alone waits on the copy's mbarrier, with a bound
+// (bt.wait_tries); the outcome goes through shared memory so that every
+// thread takes the same branch.
+// Expired waits set bt.work[2] (the host reports GATO_ERR_TIMEOUT; the
+// results of that launch are not valid) and never leave a copy in flight:
+//   - S / P^-1: thread 0 waits again, with PCG_STAGE_DRAIN_TRIES, for the
+//     copies it issued to land, then the CTA ends;
+//   - A_k / Qi_k (bt.wait_tries_dz): the threads that gave up read global
+//     memory, the CTA issues no further step-recovery copies (no re-arm of
+//     a barrier whose phase may be pending, no parity flip for a phase not
+//     seen complete), and before the CTA ends thread 0 waits for the last
+//     such copy it issued and did not see land.
 template <int NQ>
 struct PcgStage {
     __host__ __device__ static size_t matrix_floats(int N) { return (size_t)12 * N * NQ * NQ; }
@@ -982,7 +1013,8 @@ struct PcgStage {
     }
 };
 
-constexpr int PCG_STAGE_WAIT_TRIES = 1 << 22;
+constexpr int PCG_STAGE_WAIT_TRIES = 1 << 22;   // default bound: seconds
+constexpr int PCG_STAGE_DRAIN_TRIES = 1 << 22;
 
 template <int NQ, typename Acc>
 __global__ void __launch_bounds__(RowPcg<NQ, 2>::MAX_THREADS, 1)
@@ -990,7 +1022,7 @@ __global__ void __launch_bounds__(RowPcg<NQ, 2>::MAX_THREADS, 1)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];  // stage offset 128-aligned
     __shared__ __align__(8) uint64_t bar, bar_dz;
-    __shared__ int s_next, s_ok;
+    __shared__ int s_next, s_ok, s_dz_dead;
     if (*bt.done) return;
     const int N = bt.N, B = bt.B, tid = threadIdx.x;
     const size_t mat = PcgStage<NQ>::matrix_floats(N);
@@ -1002,6 +1034,7 @@ __global__ void __launch_bounds__(RowPcg<NQ, 2>::MAX_THREADS, 1)
     float* stQi = stA + blk;
     const uint32_t blk_bytes = (uint32_t)(blk * sizeof(float));
     uint32_t parity_dz = 0;
+    bool dz_outstanding = false;  // thread 0: a step-recovery copy it has not seen land
     auto fetch = [&](int pb) {  // thread 0; earlier reads of the stage are behind a barrier
         fence_proxy_async_shared();
         mbar_arrive_expect_tx(&bar, 2 * bytes);
@@ -1013,38 +1046,42 @@ __global__ void __launch_bounds__(RowPcg<NQ, 2>::MAX_THREADS, 1)
         mbar_init(&bar, 1);
         mbar_init(&bar_dz, 1);
         fence_mbar_init();
+        s_dz_dead = 0;
         if (b < B) fetch(b);
     }
     uint32_t parity = 0;
     while (b < B) {
         __syncthreads();  // the previous problem is done with the vectors and s_next
-        if (tid == 0) {
-            int i = 0;
-            while (!mbar_try_wait(&bar, parity) && ++i < PCG_STAGE_WAIT_TRIES) {
-            }
-            s_ok = i < PCG_STAGE_WAIT_TRIES;
-        }
+        if (tid == 0) s_ok = mbar_wait_bounded(&bar, parity, bt.wait_tries);
         __syncthreads();
         if (!s_ok) {
-            if (tid == 0) atomicExch(bt.work + 2, 1);
+            if (tid == 0) {
+                atomicExch(bt.work + 2, 1);
+                mbar_wait_bounded(&bar, parity, PCG_STAGE_DRAIN_TRIES);  // let the copies land
+            }
             break;
         }
         if (tid != 0) mbar_try_wait(&bar, parity);  // phase complete: acquires the data
         parity ^= 1;
-        if (dz_stage && tid == 0) {  // the previous problem's dz reads are behind a barrier
+        // a step-recovery wait that expired (any thread, previous problem,
+        // behind the barrier above) turns the step-recovery copies off
+        const bool dz_on = dz_stage && !s_dz_dead;
+        if (dz_on && tid == 0) {  // the previous problem's dz reads are behind a barrier
             fence_proxy_async_shared();
             mbar_arrive_expect_tx(&bar_dz, 2 * blk_bytes);
             bulk_copy_g2s(stA, bt.A + (size_t)b * blk, blk_bytes, &bar_dz);
             bulk_copy_g2s(stQi, bt.Qi + (size_t)b * blk, blk_bytes, &bar_dz);
+            dz_outstanding = true;
         }
         auto dz_ready = [&]() {
-            if (!dz_stage) return false;
-            int i = 0;
-            while (!mbar_try_wait(&bar_dz, parity_dz) && ++i < PCG_STAGE_WAIT_TRIES) {
+            if (!dz_on) return false;
+            if (mbar_wait_bounded(&bar_dz, parity_dz, bt.wait_tries_dz)) {
+                parity_dz ^= 1;
+                if (tid == 0) dz_outstanding = false;
+                return true;
             }
-            parity_dz ^= 1;
-            if (i < PCG_STAGE_WAIT_TRIES) return true;
             atomicExch(bt.work + 2, 1);
+            s_dz_dead = 1;
             return false;
         };
         auto next = [&]() {
@@ -1059,6 +1096,7 @@ __global__ void __launch_bounds__(RowPcg<NQ, 2>::MAX_THREADS, 1)
         __syncthreads();
         b = s_next;
     }
+    if (tid == 0 && dz_outstanding) mbar_wait_bounded(&bar_dz, parity_dz, PCG_STAGE_DRAIN_TRIES);
     if (tid == 0 && atomicAdd(bt.work + 1, 1) == (int)gridDim.x - 1) {
         bt.work[0] = 0;  // last CTA out: ready for the next launch
         bt.work[1] = 0;
@@ -1101,6 +1139,7 @@ __device__ __forceinline__ void check_body(const Batch<NQ, T>& bt)
     for (int b = threadIdx.x; b < bt.B; b += blockDim.x) {
         int cv = bt.conv[b];
         int si = bt.sqp_iters[b];
+        if (!cv && bt.pcg_iters[b] >= bt.max_pcg_iters) bt.status[b] |= GATO_STATUS_PCG_MAX_ITER;
         if (bt.pcg_iters[b] == 0) {
             cv = 1;
             si += 1;

@@ -103,6 +103,7 @@ int enqueue_mixed(gato_mixed* mx, cudaStream_t st, void* const* xu, const void* 
         CK(cudaMemsetAsync(s->sqp_iters, 0, sizeof(int) * s->B, st));
         CK(cudaMemsetAsync(s->done, 0, sizeof(int), st));
         CK(cudaMemsetAsync(s->ls_count, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(s->status, 0, sizeof(int) * s->B, st));
         nmax = std::max(nmax, s->N);
         if (rows_fit<T>(s)) {
             const size_t by = s->nq == 7 ? RowPcg<7, RPT>::template smem_bytes<T>(s->N)
@@ -366,7 +367,7 @@ int gato_mixed_stats(gato_mixed_t* mx, int c, gato_stats_t* stats)
     CK(cudaMemcpy(&rows, s->ls_count, sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(hsqp.data(), s->sqp_iters, sizeof(int) * B, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(hconv.data(), s->conv, sizeof(int) * B, cudaMemcpyDeviceToHost));
-    return read_stats(s, hsqp.data(), hconv.data(), rows, stats);
+    return read_stats(s, hsqp.data(), hconv.data(), nullptr, rows, stats);
 }
 
 int gato_mixed_elapsed_ms(gato_mixed_t* mx, float* ms)

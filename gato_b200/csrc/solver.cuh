@@ -191,8 +191,9 @@ struct gato_solver {
     double *merit_terms = nullptr, *merit_init = nullptr, *merit_init0 = nullptr,
            *merit_final = nullptr;
     int *pcg_iters = nullptr, *conv = nullptr, *sqp_iters = nullptr, *done = nullptr,
-        *ls_count = nullptr, *h_pcg = nullptr;
+        *ls_count = nullptr, *h_pcg = nullptr, *status = nullptr;
     int* work = nullptr;  // [4]: counters and wait flag of the persistent PCG
+    int wait_tries = PCG_STAGE_WAIT_TRIES, wait_tries_dz = PCG_STAGE_WAIT_TRIES;
     float *h_ls_min = nullptr, *h_ls_step = nullptr;
     // adjoint work buffers, allocated by the first gato_adjoint call
     void *adj_lam = nullptr, *adj_mu = nullptr, *adj_v = nullptr, *adj_scale = nullptr,
@@ -321,6 +322,9 @@ Batch<Tg::NQ, typename Tg::T> make_batch(gato_solver* s, void* xu, const void* x
     b.done = s->done;
     b.work = s->work;
     b.ls_count = s->ls_count;
+    b.status = s->status;
+    b.wait_tries = s->wait_tries;
+    b.wait_tries_dz = s->wait_tries_dz;
     b.h_pcg = s->h_pcg;
     b.h_ls_min = s->h_ls_min;
     b.h_ls_step = s->h_ls_step;
@@ -394,7 +398,7 @@ int launch_merit_sum(gato_solver* s, cudaStream_t st, double* out, double* out2)
 {
     ProfScope ps_(s, st, GATO_KERNEL_MERIT_SUM);
     k_merit_sum<typename Tg::Acc><<<cdiv(s->B, 128), 128, 0, st>>>(s->B, s->N, s->merit_terms,
-                                                                    out, out2);
+                                                                    out, out2, s->status);
     CKL();
     return GATO_OK;
 }
@@ -649,13 +653,15 @@ int configure_kernels(gato_solver* s)
 // host convergence check after every PCG.
 template <class Tg>
 int solve_plain(gato_solver* s, cudaStream_t st, void* xu, const void* xs, const void* goal,
-                int* host_sqp, int* host_conv, int* ls_rows)
+                int* host_sqp, int* host_conv, int* host_status, int* ls_rows)
 {
     const int B = s->B, N = s->N;
     const Dims<Tg::NQ> d{N};
     auto bt = make_batch<Tg>(s, xu, xs, goal);
     CK(cudaMemsetAsync(s->dz, 0, s->esz * (size_t)B * d.traj(), st));
     CK(cudaMemsetAsync(s->conv, 0, sizeof(int) * B, st));
+    CK(cudaMemsetAsync(s->status, 0, sizeof(int) * B, st));
+    std::fill(host_status, host_status + B, 0);
     RC(launch_merit<Tg>(s, st, bt, 1, 0, 0));
     RC(launch_merit_sum<Tg>(s, st, s->merit_init, s->merit_init0));
     std::fill(host_sqp, host_sqp + B, 0);
@@ -670,6 +676,8 @@ int solve_plain(gato_solver* s, cudaStream_t st, void* xu, const void* xs, const
         CK(cudaStreamSynchronize(st));
         int solved = 0;
         for (int b = 0; b < B; ++b) {
+            if (!host_conv[b] && s->pin_i[b] >= s->params.max_pcg_iters)
+                host_status[b] |= GATO_STATUS_PCG_MAX_ITER;
             if (s->pin_i[b] == 0) {
                 host_conv[b] = 1;
                 host_sqp[b] += 1;
@@ -703,6 +711,7 @@ int enqueue_fused(gato_solver* s, cudaStream_t st, void* xu, const void* xs, con
     CK(cudaMemsetAsync(s->sqp_iters, 0, sizeof(int) * B, st));
     CK(cudaMemsetAsync(s->done, 0, sizeof(int), st));
     CK(cudaMemsetAsync(s->ls_count, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(s->status, 0, sizeof(int) * B, st));
     RC(launch_merit_ls<Tg>(s, st, bt, 0, 0));
     for (int it = 0; it < s->params.max_sqp_iters; ++it) {
         RC(launch_fused_iter<Tg>(s, st, bt, it));
@@ -762,10 +771,18 @@ int check_device_waits(gato_solver* s)
     return GATO_OK;
 }
 
-int read_stats(gato_solver* s, const int* hsqp, const int* hconv, int rows, gato_stats_t* stats)
+// hstat: status bits found on the host (plain form) or null
+int read_stats(gato_solver* s, const int* hsqp, const int* hconv, const int* hstat, int rows,
+               gato_stats_t* stats)
 {
     RC(check_device_waits(s));
     const int B = s->B;
+    if (stats->status) {
+        CK(cudaMemcpy(stats->status, s->status, sizeof(int) * B, cudaMemcpyDeviceToHost));
+        for (int b = 0; b < B; ++b)
+            stats->status[b] |= (hstat ? hstat[b] : 0) |
+                                (hconv[b] ? GATO_STATUS_CONVERGED : GATO_STATUS_MAX_ITER);
+    }
     const int iters = std::max(1, s->params.max_sqp_iters);
     float ms = 0.0f;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
@@ -799,11 +816,11 @@ int do_solve(gato_solver* s, cudaStream_t st, void* xu, const void* xs, const vo
              gato_stats_t* stats)
 {
     const int B = s->B;
-    std::vector<int> hsqp(B), hconv(B);
+    std::vector<int> hsqp(B), hconv(B), hstat(B, 0);
     int rows = 0;
     CK(cudaEventRecord(s->ev0, st));
     if (s->form == GATO_FORM_PLAIN)
-        RC(solve_plain<Tg>(s, st, xu, xs, goal, hsqp.data(), hconv.data(), &rows));
+        RC(solve_plain<Tg>(s, st, xu, xs, goal, hsqp.data(), hconv.data(), hstat.data(), &rows));
     else
         RC(solve_fused<Tg>(s, st, xu, xs, goal));
     CK(cudaEventRecord(s->ev1, st));
@@ -814,7 +831,7 @@ int do_solve(gato_solver* s, cudaStream_t st, void* xu, const void* xs, const vo
         CK(cudaMemcpy(hsqp.data(), s->sqp_iters, sizeof(int) * B, cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(hconv.data(), s->conv, sizeof(int) * B, cudaMemcpyDeviceToHost));
     }
-    return read_stats(s, hsqp.data(), hconv.data(), rows, stats);
+    return read_stats(s, hsqp.data(), hconv.data(), hstat.data(), rows, stats);
 }
 
 // --- adjoint ---------------------------------------------------------------------

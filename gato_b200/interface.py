@@ -129,12 +129,12 @@ class BSQP:
             sqp_iters=np.zeros(B, np.int32), kkt_converged=np.zeros(B, np.int32),
             final_merit=np.zeros(B, np.float32), initial_merit=np.zeros(B, np.float32),
             pcg_iters=np.zeros(it * B, np.int32), ls_min_merit=np.zeros(it * B, np.float32),
-            ls_step_size=np.zeros(it * B, np.float32))
+            ls_step_size=np.zeros(it * B, np.float32), status=np.zeros(B, np.int32))
         st = L.GatoStats(
             0.0, 0, L.iptr(bufs["sqp_iters"]), L.iptr(bufs["kkt_converged"]),
             L.fptr(bufs["final_merit"]), L.fptr(bufs["initial_merit"]),
             L.iptr(bufs["pcg_iters"]), L.fptr(bufs["ls_min_merit"]),
-            L.fptr(bufs["ls_step_size"]))
+            L.fptr(bufs["ls_step_size"]), L.iptr(bufs["status"]))
         return st, bufs
 
     def solve_raw(self, xu, dt, x_s, reference_traj):
@@ -166,6 +166,7 @@ class BSQP:
             "pcg_iters": bufs["pcg_iters"][: n * B].reshape(n, B),
             "ls_min_merit": bufs["ls_min_merit"][: n * B].reshape(n, B),
             "ls_step_size": bufs["ls_step_size"][: n * B].reshape(n, B),
+            "status": bufs["status"],
         }
 
     def solve(self, xcur_B, eepos_goals_B, XU_B=None):
@@ -194,6 +195,7 @@ class BSQP:
         s["pcg_times_us"] = result["pcg_times_us"]
         s["min_merit"] = result["ls_min_merit"]
         s["step_size"] = result["ls_step_size"]
+        s["status"] = result["status"]
         mm = s["min_merit"]
         if mm.size and mm.ndim == 2:
             best = np.min(mm.astype(np.float32), axis=1)
@@ -226,6 +228,7 @@ class BSQP:
             "pcg_iters": bufs["pcg_iters"][: n * B].reshape(n, B),
             "ls_min_merit": bufs["ls_min_merit"][: n * B].reshape(n, B),
             "ls_step_size": bufs["ls_step_size"][: n * B].reshape(n, B),
+            "status": bufs["status"],
         }
 
     def adjoint_device(self, d_xu, d_xs, d_goal, d_dl, stream=0, tol=0.0, max_iters=0,
@@ -319,6 +322,12 @@ class BSQP:
         qd[:, nq:] = self.params.qd_cost
         rd = np.full((B, self.nu), self.params.u_cost, np.float32)
         return qd, rd
+
+    def set_wait_limits(self, copy_tries=-1, step_copy_tries=-1):
+        """Bounds of the persistent PCG's device waits for its bulk copies
+        (gato_set_wait_limits): -1 restores the default, 0 gives up at once
+        (the next solve then raises GatoError with GATO_ERR_TIMEOUT)."""
+        L.check(L.load().gato_set_wait_limits(self._h, int(copy_tries), int(step_copy_tries)))
 
     def set_rho_adaptation(self, enabled):
         L.check(L.load().gato_set_rho_adaptation(self._h, int(bool(enabled))))

@@ -89,7 +89,8 @@ class MixedBSQP:
         return {"sqp_iters": bufs["sqp_iters"], "kkt_converged": bufs["kkt_converged"],
                 "pcg_iters": bufs["pcg_iters"][: n * B].reshape(n, B), "ls_num_iters": n,
                 "final_merit": bufs["final_merit"], "initial_merit": bufs["initial_merit"],
-                "ls_step_size": bufs["ls_step_size"][: n * B].reshape(n, B)}
+                "ls_step_size": bufs["ls_step_size"][: n * B].reshape(n, B),
+                "status": bufs["status"]}
 
     def config(self, lanes_per_knot=16, problems_per_block=1, ctas_per_sm=2):
         L.check(L.load().gato_mixed_config(self._h, int(lanes_per_knot), int(problems_per_block),

@@ -114,6 +114,24 @@ typedef struct gato_params {
     double rho;
 } gato_params_t;
 
+/* Per-problem status word of a solve (gato_stats_t.status), a bit set.  The
+   reference reports only kkt_converged, step_size = -1 on a failed line
+   search and its rho reset (gato/bsqp/kernels/line_search.cuh:75-81,
+   gato/bsqp/bsqp.cuh:153-156); these bits add what a caller needs to tell a
+   failed problem from a slow one. */
+enum {
+    GATO_STATUS_CONVERGED = 1,    /* a PCG took zero iterations: the
+                                     reference's kkt_converged */
+    GATO_STATUS_MAX_ITER = 2,     /* the solve ended with the problem not
+                                     converged (SQP iterations exhausted, or
+                                     the batch stopped at solve_ratio) */
+    GATO_STATUS_LS_FAIL = 4,      /* at least one line search found no step
+                                     size that lowered the merit (step -1) */
+    GATO_STATUS_NONFINITE = 8,    /* a non-finite merit: the problem's state,
+                                     or every trial step of a line search */
+    GATO_STATUS_PCG_MAX_ITER = 16 /* at least one PCG ran to max_pcg_iters */
+};
+
 /* Per-solve statistics, all host memory supplied by the caller; any pointer
    may be NULL.  Replaces the dict built in python/bindings.cu:96-147.
    Arrays indexed [iteration][problem] hold max_sqp_iters*B entries; the first
@@ -128,6 +146,8 @@ typedef struct gato_stats {
     int32_t* pcg_iters;      /* [max_sqp_iters][B] */
     float* ls_min_merit;     /* [max_sqp_iters][B] */
     float* ls_step_size;     /* [max_sqp_iters][B] */
+    int32_t* status;         /* [B] GATO_STATUS_* bits (no counterpart in
+                                the reference's dict) */
 } gato_stats_t;
 
 typedef struct gato_solver gato_solver_t;
@@ -226,6 +246,18 @@ int gato_set_pcg_tol_batch(gato_solver_t* s, const float* h_tol);
 /* Sets the time step used by gato_solve (gato_solve_host takes it per call,
    as PyBSQP::solve does). */
 int gato_set_dt(gato_solver_t* s, float dt);
+
+/* Bounds of the device-side waits of the persistent FP32 PCG (no
+   counterpart in the reference, which has no bulk copies): how many
+   mbarrier try_wait calls (each suspends the waiting thread for at most about
+   a microsecond) a CTA makes before it gives up on a problem's S / P^-1
+   copy (copy_tries) and on the step recovery's A_k / Qi_k copy
+   (step_copy_tries).  A wait that gives up lets the copies in flight land,
+   and the next synchronising call on the handle returns GATO_ERR_TIMEOUT
+   (the results of that solve are not valid).  A negative value restores
+   the default (about four million tries: seconds); 0 gives up at once, which
+   is how the tests exercise this path. */
+int gato_set_wait_limits(gato_solver_t* s, int copy_tries, int step_copy_tries);
 
 /* Zeroes the dual warm start.  Replaces BSQP::reset_dual (bsqp.cuh:85). */
 int gato_reset_dual(gato_solver_t* s);

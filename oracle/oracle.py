@@ -133,7 +133,7 @@ def _load():
         "orc_solver_set_lambda": (None, [vp, _dp]),
         "orc_solver_get_rho": (None, [vp, _dp]),
         "orc_solver_solve": (ctypes.c_int, [vp, ctypes.c_double, _dp, _dp, _dp, _ip, _ip, _dp,
-                                            _dp, _ip, _dp, _dp, _dp]),
+                                            _dp, _ip, _dp, _dp, _dp, _ip]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -379,13 +379,15 @@ class Solver:
         lsm = np.zeros(max(it, 1) * B)
         lss = np.zeros(max(it, 1) * B)
         secs = ctypes.c_double(0)
+        status = np.zeros(B, np.int32)
         n = lib().orc_solver_solve(self.h, dt, _p(xu), _p(xs), _p(goal), _ip_(sqp), _ip_(conv),
                                    _p(fm), _p(im), _ip_(pcg_it), _p(lsm), _p(lss),
-                                   ctypes.byref(secs))
+                                   ctypes.byref(secs), _ip_(status))
         stats = dict(sqp_iters=sqp, kkt_converged=conv, final_merit=fm, initial_merit=im,
                      ls_num_iters=n, pcg_iters=pcg_it[: n * B].reshape(n, B),
                      ls_min_merit=lsm[: n * B].reshape(n, B),
-                     ls_step_size=lss[: n * B].reshape(n, B), seconds=secs.value)
+                     ls_step_size=lss[: n * B].reshape(n, B), seconds=secs.value,
+                     status=status)
         return xu, stats
 
 

@@ -1064,9 +1064,12 @@ static void round_f32(double* p, size_t n)
     for (size_t i = 0; i < n; ++i) p[i] = (double)(float)p[i];
 }
 
+/* per-problem status bits, the GATO_STATUS_* values of include/gato_b200.h */
+enum { ST_CONVERGED = 1, ST_MAX_ITER = 2, ST_LS_FAIL = 4, ST_NONFINITE = 8, ST_PCG_MAX = 16 };
+
 struct SolveOut {
     int ls_num_iters;
-    std::vector<int> sqp_iters, kkt_converged, pcg_iters;
+    std::vector<int> sqp_iters, kkt_converged, pcg_iters, status;
     std::vector<double> final_merit, initial_merit, ls_min_merit, ls_step_size;
 };
 
@@ -1085,7 +1088,7 @@ static void solve(Solver& S, double dt, double* xu, const double* xs, const doub
         r(Bn * N * nu), A(Bn * N * nx * nx), Bm(Bn * N * nx * nu), c(Bn * N * nx),
         Sm(Bn * d.b3d()), Pi(Bn * d.b3d()), gam(Bn * L), dz(Bn * T, 0.0), merit_init(Bn),
         merit_a(Bn * NUM_ALPHAS);
-    std::vector<int> conv(Bn, 0), sqp_it(Bn, 0), pcg_it(Bn, 0);
+    std::vector<int> conv(Bn, 0), sqp_it(Bn, 0), pcg_it(Bn, 0), status(Bn, 0);
     out.pcg_iters.clear();
     out.ls_min_merit.clear();
     out.ls_step_size.clear();
@@ -1097,6 +1100,8 @@ static void solve(Solver& S, double dt, double* xu, const double* xs, const doub
                               goal + b * 6 * N, fext_of(b));
     });
     out.initial_merit = merit_init;
+    for (int b = 0; b < Bn; ++b)
+        if (!std::isfinite(merit_init[b])) status[b] |= ST_NONFINITE;
     for (int it = 0; it < P.max_sqp_iters; ++it) {
         parallel_for(nthr, Bn, [&](int b) {
             double* Qb = &Q[b * N * nx * nx];
@@ -1135,6 +1140,7 @@ static void solve(Solver& S, double dt, double* xu, const double* xs, const doub
         out.pcg_iters.insert(out.pcg_iters.end(), pcg_it.begin(), pcg_it.end());
         int num_solved = 0;
         for (int b = 0; b < Bn; ++b) {
+            if (!conv[b] && pcg_it[b] >= P.max_pcg_iters) status[b] |= ST_PCG_MAX;
             if (pcg_it[b] == 0) {
                 conv[b] = 1;
                 sqp_it[b] += 1;
@@ -1157,6 +1163,10 @@ static void solve(Solver& S, double dt, double* xu, const double* xs, const doub
             }
             /* lineSearchAndUpdateBatchedKernel (line_search.cuh:27-97) */
             bool ok = best < merit_init[b];
+            bool any_finite = false;
+            for (int j = 0; j < NUM_ALPHAS; ++j) any_finite |= std::isfinite(merit_a[b * NUM_ALPHAS + j]);
+            if (!ok) status[b] |= ST_LS_FAIL;
+            if (!any_finite) status[b] |= ST_NONFINITE;
             if (S.adapt_rho) {
                 double mult = ok ? std::min(S.drho[b] / RHO_FACTOR, 1.0 / RHO_FACTOR)
                                  : std::max(S.drho[b] * RHO_FACTOR, RHO_FACTOR);
@@ -1187,6 +1197,11 @@ static void solve(Solver& S, double dt, double* xu, const double* xs, const doub
     out.final_merit = merit_init;
     out.sqp_iters = sqp_it;
     out.kkt_converged = conv;
+    for (int b = 0; b < Bn; ++b) {
+        if (!std::isfinite(merit_init[b])) status[b] |= ST_NONFINITE;
+        status[b] |= conv[b] ? ST_CONVERGED : ST_MAX_ITER;
+    }
+    out.status = status;
     S.drho = S.drho_init;
 }
 
@@ -1396,12 +1411,12 @@ void orc_solver_get_rho(void* h, double* out)
 
 /* Runs one solve.  Outputs (may be NULL): sqp_iters[B], kkt_converged[B],
    final_merit[B], initial_merit[B], pcg_iters[max_iters*B],
-   ls_min_merit[max_iters*B], ls_step_size[max_iters*B]; returns ls_num_iters;
-   *seconds gets the wall time of the solve. */
+   ls_min_merit[max_iters*B], ls_step_size[max_iters*B], status[B]; returns
+   ls_num_iters; *seconds gets the wall time of the solve. */
 int orc_solver_solve(void* h, double dt, double* xu, const double* xs, const double* goal,
                      int* sqp_iters, int* kkt_converged, double* final_merit,
                      double* initial_merit, int* pcg_iters, double* ls_min_merit,
-                     double* ls_step_size, double* seconds)
+                     double* ls_step_size, double* seconds, int* status)
 {
     Solver* S = (Solver*)h;
     SolveOut out;
@@ -1418,6 +1433,7 @@ int orc_solver_solve(void* h, double dt, double* xu, const double* xs, const dou
     if (pcg_iters) memcpy(pcg_iters, out.pcg_iters.data(), sizeof(int) * Bn * nrows);
     if (ls_min_merit) memcpy(ls_min_merit, out.ls_min_merit.data(), sizeof(double) * Bn * nrows);
     if (ls_step_size) memcpy(ls_step_size, out.ls_step_size.data(), sizeof(double) * Bn * nrows);
+    if (status) memcpy(status, out.status.data(), sizeof(int) * Bn);
     return nrows;
 }
 

@@ -93,9 +93,10 @@ def test_rollout_backward_is_the_composition_of_step_adjoints(oracle_mod):
     import ctypes
     import gato_b200._lib as L
     rho_after = s.get_rho().copy()
+    d_dl = T(dl)  # held in a name for the duration of the call
     L.check(L.load().gato_rollout_backward(
         s._h, None, STEPS, L.vptr(out["goal_traj"]), L.vptr(out["x"]), L.vptr(out["u"]),
-        L.vptr(out["ckpt_xu"]), L.vptr(out["ckpt_rho"]), L.vptr(T(dl)), L.vptr(g_x0),
+        L.vptr(out["ckpt_xu"]), L.vptr(out["ckpt_rho"]), L.vptr(d_dl), L.vptr(g_x0),
         L.vptr(g_goal), L.vptr(g_w), 0.0, 0))
     torch.cuda.synchronize()
     np.testing.assert_allclose(s.get_rho(), rho_after, rtol=0, atol=0)

@@ -25,8 +25,12 @@ def _schur_system(torch, L, h, pr, nq, N, B):
     S, Pi = z(B, N, 3 * nx * nx), z(B, N, 3 * nx * nx)
     gam = z(B, (N + 2) * nx)
     lib = L.load()
-    L.check(lib.gato_stage_setup_kkt(h, None, V(t(pr["xu"])), V(t(pr["xs"])), V(t(pr["goal"])),
+    # inputs held in names: a temporary freed inside the argument list could
+    # hand its memory to the next input before the kernel reads it
+    d_xu, d_xs, d_goal = t(pr["xu"]), t(pr["xs"]), t(pr["goal"])
+    L.check(lib.gato_stage_setup_kkt(h, None, V(d_xu), V(d_xs), V(d_goal),
                                      V(Q), V(R), V(q), V(r), V(A), V(Bm), V(c)))
+    torch.cuda.synchronize()
     L.check(lib.gato_stage_form_schur(h, None, V(Q), V(R), V(q), V(r), V(A), V(Bm), V(c),
                                       V(S), V(Pi), V(gam)))
     return S, Pi, gam
