@@ -140,6 +140,12 @@ SIGNATURES = {
                                     ctypes.c_double, ctypes.c_int, _vp]),
     "gato_adjoint_f64": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                         ctypes.c_double, ctypes.c_int, _vp]),
+    "gato_qp_step": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_double,
+                                    ctypes.c_int, _vp]),
+    "gato_qp_step_f64": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_double,
+                                        ctypes.c_int, _vp]),
+    "gato_select_hypothesis": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_double, _vp,
+                                              _vp, _vp]),
     "gato_pcg_static": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_float, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
 }

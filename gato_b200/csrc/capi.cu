@@ -442,6 +442,38 @@ int gato_sim_forward(gato_solver_t* s, const float* h_xk, const float* h_uk, flo
     return GATO_OK;
 }
 
+int gato_select_hypothesis(gato_solver_t* s, void* stream, const void* d_x_last,
+                           const void* d_u_last, const void* d_x_curr, double dt, void* d_xu,
+                           void* d_err, int32_t* d_best)
+{
+    RC(check_handle(s));
+    if (!d_x_last || !d_u_last || !d_x_curr || !d_err || !d_best)
+        return fail(GATO_ERR_ARG, "null device buffer");
+    if (!(dt > 0.0)) return fail(GATO_ERR_ARG, "dt must be positive");
+    RC(bind_device(s));
+    cudaStream_t st = as_stream(stream);
+    return dispatch(s, [&](auto tg) {
+        using Tg = decltype(tg);
+        using T = typename Tg::T;
+        const size_t sm = WPB * DynSmem<Tg::NQ>::SIZE * sizeof(T);
+        k_hyp_error<Tg::NQ, T><<<cdiv(s->B, WPB), WPB * WARP, sm, st>>>(
+            dmodel<Tg>(s), s->B, (T)dt, (const T*)d_x_last, (const T*)d_u_last,
+            (const T*)d_x_curr, (const T*)s->fext, s->use_fext, (T*)d_err);
+        CKL();
+        k_hyp_argmin<T><<<1, 1024, 0, st>>>(s->B, (const T*)d_err, d_best);
+        CKL();
+        if (d_xu) {
+            const int traj = (3 * s->nq) * s->N - s->nq;
+            const size_t n = (size_t)s->B * traj;
+            const int grid = (int)std::min<size_t>(cdiv((int)std::min<size_t>(n, 1u << 30), 256),
+                                                   4 * (size_t)s->nsm);
+            k_hyp_broadcast<T><<<grid, 256, 0, st>>>(s->B, traj, d_best, (T*)d_xu);
+            CKL();
+        }
+        return (int)GATO_OK;
+    });
+}
+
 // --- stage entry points (single-precision solvers) ---------------------------
 int gato_stage_setup_kkt(gato_solver_t* s, void* stream, const float* d_xu, const float* d_xs,
                          const float* d_goal, float* d_Q, float* d_R, float* d_q, float* d_r,
@@ -501,6 +533,37 @@ int gato_stage_pcg(gato_solver_t* s, void* stream, const float* d_S, const float
         bt.pcg_iters = d_iters;
         return launch_pcg<Tg>(s, st, bt, -1);
     });
+}
+
+static int qp_step_any(gato_solver_t* s, void* stream, void* d_xu, const void* d_xs,
+                       const void* d_goal, void* d_dz, double tol, int max_iters,
+                       int32_t* h_iters)
+{
+    if (!d_xu || !d_xs || !d_goal || !d_dz) return fail(GATO_ERR_ARG, "null device buffer");
+    RC(bind_device(s));
+    if (tol < 0) tol = (double)s->params.pcg_tol;
+    if (max_iters <= 0) max_iters = s->params.max_pcg_iters;
+    return dispatch(s, [&](auto tg) {
+        return qp_step_impl<decltype(tg)>(s, as_stream(stream), d_xu, d_xs, d_goal, d_dz, tol,
+                                          max_iters, h_iters);
+    });
+}
+
+int gato_qp_step(gato_solver_t* s, void* stream, const float* d_xu, const float* d_xs,
+                 const float* d_goal, float* d_dz, double tol, int max_iters, int32_t* h_iters)
+{
+    RC(check_handle(s));
+    RC(check_single(s));
+    return qp_step_any(s, stream, (void*)d_xu, d_xs, d_goal, d_dz, tol, max_iters, h_iters);
+}
+
+int gato_qp_step_f64(gato_solver_t* s, void* stream, const double* d_xu, const double* d_xs,
+                     const double* d_goal, double* d_dz, double tol, int max_iters,
+                     int32_t* h_iters)
+{
+    RC(check_handle(s));
+    RC(check_double(s));
+    return qp_step_any(s, stream, (void*)d_xu, d_xs, d_goal, d_dz, tol, max_iters, h_iters);
 }
 
 int gato_adjoint(gato_solver_t* s, void* stream, const float* d_xu, const float* d_xs,

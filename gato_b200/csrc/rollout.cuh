@@ -185,4 +185,95 @@ __global__ void k_goal_accum(T* __restrict__ g_traj, const T* __restrict__ g, in
     g_traj[(size_t)b * stride + 6 * t + j] += g[i];
 }
 
+// ------------------------------------------------------------------ hypotheses
+// Batch-hypothesis selection of the reference's MPC loop
+// (python/bsqp/mpc_controller.py:295-309 evaluate_best_trajectory, 241-242):
+// problem b simulates (x_last, u_last) for one dt under its own wrench
+// hypothesis f_ext[b] and scores err[b] = |x_b - x_curr|_2; the smallest
+// error wins and its trajectory becomes every problem's warm start.
+// One warp per problem; the squared differences are summed in FP64.
+template <int NQ, typename T>
+__global__ void k_hyp_error(DevModel<NQ, T> M, int B, T dt, const T* __restrict__ x_last,
+                            const T* __restrict__ u_last, const T* __restrict__ x_curr,
+                            const T* fext, int use_fext, T* __restrict__ err)
+{
+    constexpr int nx = 2 * NQ;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
+    const int b = blockIdx.x * (blockDim.x / WARP) + warp_id();
+    if (b >= B) return;
+    T* s = smem + warp_id() * DynSmem<NQ>::SIZE;
+    const T* q = x_last;
+    const T* qd = x_last + NQ;
+    dyn_load_transforms<NQ, T>(M, q, s);
+    __syncwarp();
+    T mc[NQ];
+    dyn_forward<NQ, T>(M, s, q, qd, u_last, use_fext ? fext + 6 * b : nullptr, false, mc);
+    const int l = lane_id();
+    double d2 = 0.0;
+    if (l < nx) {
+        T v;
+        if (l < NQ)
+            v = q[l] + dt * qd[l] + T(0.5) * s[DynSmem<NQ>::QDD + l] * dt * dt;
+        else
+            v = qd[l - NQ] + dt * s[DynSmem<NQ>::QDD + l - NQ];
+        const double d = (double)v - (double)x_curr[l];
+        d2 = d * d;
+    }
+    d2 = warp_sum(d2);
+    if (l == 0) err[b] = (T)sqrt(d2);
+}
+
+// numpy.argmin order: a NaN counts as the smallest value, ties go to the
+// lower index
+template <typename T>
+__device__ __forceinline__ bool hyp_before(T a, int ia, T b, int ib)
+{
+    const bool na = isnan((double)a), nb = isnan((double)b);
+    if (na != nb) return na;
+    if (!na && a != b) return a < b;
+    return ia < ib;
+}
+
+// one block: best[0] = argmin_b err[b]
+template <typename T>
+__global__ void k_hyp_argmin(int B, const T* __restrict__ err, int* __restrict__ best)
+{
+    __shared__ T sv[1024];
+    __shared__ int si[1024];
+    const int t = threadIdx.x;
+    T v = T(0);
+    int iv = -1;
+    for (int b = t; b < B; b += blockDim.x)
+        if (iv < 0 || hyp_before(err[b], b, v, iv)) {
+            v = err[b];
+            iv = b;
+        }
+    sv[t] = v;
+    si[t] = iv;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (t < w && si[t + w] >= 0 && (si[t] < 0 || hyp_before(sv[t + w], si[t + w], sv[t], si[t]))) {
+            sv[t] = sv[t + w];
+            si[t] = si[t + w];
+        }
+        __syncthreads();
+    }
+    if (t == 0) best[0] = si[0];
+}
+
+// every row of xu [B][traj] := row best[0] (the chosen trajectory as the
+// warm start of all hypotheses)
+template <typename T>
+__global__ void k_hyp_broadcast(int B, int traj, const int* __restrict__ best, T* xu)
+{
+    const int src = best[0];
+    const size_t n = (size_t)B * traj;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int b = (int)(i / traj);
+        if (b != src) xu[i] = xu[(size_t)src * traj + i % traj];
+    }
+}
+
 }  // namespace gato

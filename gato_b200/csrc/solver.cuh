@@ -2,6 +2,7 @@
 // drivers shared by the C-ABI translation units (capi.cu, mixed.cu).
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>  // header-only; a no-op unless a profiler attaches
 
 #include <algorithm>
 #include <cmath>
@@ -338,13 +339,29 @@ constexpr int LS_THREADS = 128;
 
 inline int cdiv(int a, int b) { return (a + b - 1) / b; }
 
-// Brackets one launch with events when profiling is on.
+// An NVTX range over a host scope (solve, SQP iteration, stage launch): the
+// stage structure shows in Nsight timelines.  Graph replays run no host code,
+// so there the ranges mark the capture.
+struct Nvtx {
+    explicit Nvtx(const char* name) { nvtxRangePushA(name); }
+    ~Nvtx() { nvtxRangePop(); }
+    Nvtx(const Nvtx&) = delete;
+    Nvtx& operator=(const Nvtx&) = delete;
+};
+
+const char* const KERNEL_GROUP_NAMES[GATO_KERNEL_COUNT] = {
+    "kkt", "schur", "pcg", "dz", "merit", "line_search", "fused_iter", "check", "merit_sum"};
+
+// Brackets one launch with an NVTX range named by its kernel group, and with
+// events when profiling is on.
 struct ProfScope {
     gato_solver* s;
     cudaStream_t st;
     int id;
+    Nvtx range;
     cudaEvent_t a = nullptr, b = nullptr;
-    ProfScope(gato_solver* s_, cudaStream_t st_, int id_) : s(s_), st(st_), id(id_)
+    ProfScope(gato_solver* s_, cudaStream_t st_, int id_)
+        : s(s_), st(st_), id(id_), range(KERNEL_GROUP_NAMES[id_])
     {
         if (!s->prof) return;
         cudaEventCreate(&a);
@@ -668,6 +685,7 @@ int solve_plain(gato_solver* s, cudaStream_t st, void* xu, const void* xs, const
     std::fill(host_conv, host_conv + B, 0);
     int rows = 0;
     for (int it = 0; it < s->params.max_sqp_iters; ++it) {
+        Nvtx r_("sqp_iteration");
         RC(launch_kkt<Tg>(s, st, bt));
         RC(launch_schur<Tg>(s, st, bt));
         RC(launch_pcg<Tg>(s, st, bt, it));
@@ -714,6 +732,7 @@ int enqueue_fused(gato_solver* s, cudaStream_t st, void* xu, const void* xs, con
     CK(cudaMemsetAsync(s->status, 0, sizeof(int) * B, st));
     RC(launch_merit_ls<Tg>(s, st, bt, 0, 0));
     for (int it = 0; it < s->params.max_sqp_iters; ++it) {
+        Nvtx r_("sqp_iteration");
         RC(launch_fused_iter<Tg>(s, st, bt, it));
         RC(launch_check<Tg>(s, st, bt));
         RC(launch_merit_ls<Tg>(s, st, bt, 1, it));
@@ -815,6 +834,7 @@ template <class Tg>
 int do_solve(gato_solver* s, cudaStream_t st, void* xu, const void* xs, const void* goal,
              gato_stats_t* stats)
 {
+    Nvtx r_(s->form == GATO_FORM_PLAIN ? "gato_solve(plain)" : "gato_solve(fused)");
     const int B = s->B;
     std::vector<int> hsqp(B), hconv(B), hstat(B, 0);
     int rows = 0;
@@ -894,6 +914,7 @@ int adjoint_impl(gato_solver* s, cudaStream_t st, void* xu, const void* xs, cons
     const int B = s->B, N = s->N;
     const Dims<NQ> d{N};
     constexpr int nx = Dims<NQ>::nx, nu = Dims<NQ>::nu;
+    Nvtx r_("gato_adjoint");
     RC(adj_alloc(s));
     auto bt = make_batch<Tg>(s, xu, xs, goal);
     bt.conv = s->adj_conv;
@@ -933,6 +954,45 @@ int adjoint_impl(gato_solver* s, cudaStream_t st, void* xu, const void* xs, cons
     CKL();
     if (h_iters) {
         CK(cudaMemcpyAsync(h_iters, s->adj_iters, sizeof(int) * 2 * B, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    return GATO_OK;
+}
+
+// The QP step of the SQP at xu alone: KKT blocks, Schur system, PCG from the
+// solver's lambda (left unchanged) with relative tolerance tol (0: no
+// tolerance stop, exactly max_iters iterations unless the residual is exactly
+// zero) and the step recovery, dz into dz_out.
+template <class Tg>
+int qp_step_impl(gato_solver* s, cudaStream_t st, void* xu, const void* xs, const void* goal,
+                 void* dz_out, double tol, int max_iters, int32_t* h_iters)
+{
+    using T = typename Tg::T;
+    const int B = s->B;
+    const Dims<Tg::NQ> d{s->N};
+    RC(adj_alloc(s));
+    auto bt = make_batch<Tg>(s, xu, xs, goal);
+    bt.conv = s->adj_conv;
+    bt.done = s->adj_done;
+    bt.tol = (T*)s->adj_tol;
+    bt.h_pcg = nullptr;
+    bt.max_pcg_iters = max_iters;
+    bt.abs_tol = tol > 0 ? 1e-30f : 0.0f;
+    CK(cudaMemsetAsync(s->adj_conv, 0, sizeof(int) * B, st));
+    CK(cudaMemsetAsync(s->adj_done, 0, sizeof(int), st));
+    k_fill<T><<<cdiv(B, 256), 256, 0, st>>>((T*)s->adj_tol, B, (T)tol);
+    CKL();
+    RC(launch_kkt<Tg>(s, st, bt));
+    RC(launch_schur<Tg>(s, st, bt));
+    CK(cudaMemcpyAsync(s->adj_lam, s->lambda, s->esz * (size_t)B * d.vecp(),
+                       cudaMemcpyDeviceToDevice, st));
+    auto bf = bt;
+    bf.lambda = (T*)s->adj_lam;
+    bf.pcg_iters = s->adj_iters;
+    bf.dz = (T*)dz_out;
+    RC(pcg_and_step<Tg>(s, st, bf));
+    if (h_iters) {
+        CK(cudaMemcpyAsync(h_iters, s->adj_iters, sizeof(int) * B, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
     }
     return GATO_OK;

@@ -284,6 +284,22 @@ int gato_get_rho(gato_solver_t* s, float* h_rho);
 int gato_sim_forward(gato_solver_t* s, const float* h_xk, const float* h_uk,
                      float dt, float* h_xkp1);
 
+/* Batch-hypothesis selection of the reference's MPC loop
+   (python/bsqp/mpc_controller.py:295-309 evaluate_best_trajectory and the
+   warm-start broadcast at 241-242), on the device and stream-ordered: every
+   problem b simulates (d_x_last [nx], d_u_last [nu]) for dt under its own
+   wrench hypothesis (the f_ext batch of gato_set_f_ext_batch), d_err [B]
+   receives |x_b - d_x_curr|_2 and d_best [1] the index of the smallest
+   error (numpy.argmin order: a NaN error counts as smallest, ties go to the
+   lower index); when d_xu [B][traj] is non-NULL every row is overwritten
+   with row best, the chosen trajectory as every problem's next warm start.
+   Buffers in the solver's scalar type; no host synchronisation.  The
+   reference's force-estimator update that consumes d_err stays on the host
+   (examples/force_estimator.py). */
+int gato_select_hypothesis(gato_solver_t* s, void* stream, const void* d_x_last,
+                           const void* d_u_last, const void* d_x_curr, double dt,
+                           void* d_xu, void* d_err, int32_t* d_best);
+
 /*
  * Stage-level entry points on device buffers, for parity testing and custom
  * drivers.  Layouts follow the reference's batch layouts:
@@ -309,6 +325,23 @@ int gato_stage_form_schur(gato_solver_t* s, void* stream, float* d_Q,
 int gato_stage_pcg(gato_solver_t* s, void* stream, const float* d_S,
                    const float* d_Pinv, const float* d_gamma, float* d_lambda,
                    int32_t* d_iters);
+
+/* The QP step of one SQP iteration at d_xu, without line search: KKT
+   blocks, Schur complement, PCG warm-started from the solver's lambda (which
+   is left unchanged) and step recovery; d_dz [B][traj] receives dz.  No
+   counterpart in the reference, whose step stays inside the solve
+   (gato/bsqp/bsqp.cuh:116-140); it is the map gato_adjoint differentiates,
+   exposed so that its derivative can be checked by finite differences on the
+   device.  tol: relative PCG tolerance (< 0: the solver's pcg_tol; 0: no
+   tolerance stop, every problem runs max_iters iterations unless its
+   residual reaches exactly zero); max_iters <= 0: the solver's
+   max_pcg_iters.  h_iters (optional, host [B]) receives the PCG counts. */
+int gato_qp_step(gato_solver_t* s, void* stream, const float* d_xu,
+                 const float* d_xs, const float* d_goal, float* d_dz, double tol,
+                 int max_iters, int32_t* h_iters);
+int gato_qp_step_f64(gato_solver_t* s, void* stream, const double* d_xu,
+                     const double* d_xs, const double* d_goal, double* d_dz,
+                     double tol, int max_iters, int32_t* h_iters);
 
 /* Adjoint of the converged subproblem (no counterpart in the reference).
    For a loss l of the trajectory d_xu returned by gato_solve (same x_s and

@@ -140,3 +140,28 @@ def test_autograd_function_gradients():
     assert torch.allclose(goals.grad, g_goal, rtol=1e-9, atol=1e-12)
     assert torch.allclose(logq.grad, g_w[:, :s.nx] * logq.exp(), rtol=1e-9, atol=1e-12)
     s.close()
+
+
+def test_config4_gradients_dense_and_device_differences():
+    """The differentiable-solve configuration: iiwa14 N=32, batch 256, Q/R
+    diagonals exp(u), u ~ U[-2, 2], loss |XU* - XU_target|^2.  The FP32
+    forward and adjoint with FP64 reductions (mixed) against the dense FP64
+    KKT gradient on all 256 problems; the FP64 adjoint likewise; and FP64
+    central differences (h = 1e-6) of the same QP map through the device's
+    QP step (gato_qp_step_f64) against the dense gradient on 16 problems,
+    which checks the dense reference on the device path."""
+    import os
+    import sys
+    import torch
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    torch.cuda.set_device(0)
+    r = bench.adjoint_config4(torch, torch.device("cuda"), os.cpu_count() or 1,
+                              precisions=("mixed", "fp64"))
+    fd = r["fp64"]["fd_device_vs_dense"]["rel_err"]
+    assert max(v["max"] for v in fd.values()) < 1e-4, fd
+    e64 = r["fp64"]["vs_dense_fp64"]
+    assert max(v["max"] for v in e64.values()) < 1e-5, e64
+    em = r["mixed"]["vs_dense_fp64"]
+    assert max(v["median"] for v in em.values()) < 2e-2, em
+    assert r["mixed"]["pcg_iters_max"]["adjoint"] < 4 * 32 * 7, r["mixed"]["pcg_iters_max"]

@@ -48,7 +48,8 @@ def test_mixed_solve_matches_classes_solved_alone(precision):
             c.reset_rho()
         mx.config(kg, ppb, occ)
         xu = [T(pr["xu"]) for pr in data]
-        mx.solve_device(xu, [T(pr["xs"]) for pr in data], [T(pr["goal"]) for pr in data])
+        xs, goal = [T(pr["xs"]) for pr in data], [T(pr["goal"]) for pr in data]
+        mx.solve_device(xu, xs, goal)
         torch.cuda.synchronize()
         for c, ((plant, N, B), pr) in enumerate(zip(CLASSES, data)):
             ref_xu, ref_pcg, ref_lam = _alone(plant, N, B, pr, precision, T)
@@ -83,4 +84,34 @@ def test_mixed_tuner_picks_a_shape_and_restores_state():
         np.testing.assert_array_equal(c.get_lambda(), l)
     mx.solve_device(xu, xs, goal)
     assert mx.elapsed_ms() > 0
+    mx.close()
+
+
+ORACLE_CLASSES = [("indy7", 128, 3), ("iiwa14", 64, 2), ("iiwa14", 32, 3), ("indy7", 8, 4)]
+
+
+def test_fp64_mixed_solve_reproduces_oracle(oracle_mod):
+    """One FP64 mixed solve over four classes, the N = 128 class (cluster
+    PCG on a parallel graph branch) among them: every class reproduces the
+    FP64 oracle run on the same problems (iteration counts, line-search
+    steps, trajectories to 1e-8)."""
+    import torch
+    from gato_b200.mixed import MixedBSQP
+    torch.cuda.set_device(0)
+    O = oracle_mod
+    T = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+    data = [problem(plant, N, B, seed=80 + i) for i, (plant, N, B) in enumerate(ORACLE_CLASSES)]
+    mx = MixedBSQP(ORACLE_CLASSES, precision="fp64", **PARAMS_CFG2)
+    xu = [T(pr["xu"]) for pr in data]
+    xs, goal = [T(pr["xs"]) for pr in data], [T(pr["goal"]) for pr in data]
+    mx.solve_device(xu, xs, goal)
+    torch.cuda.synchronize()
+    for c, ((plant, N, B), pr) in enumerate(zip(ORACLE_CLASSES, data)):
+        ref = O.Solver(plant, N, B, O.make_params(dt=0.01, **PARAMS_CFG2), threads=4)
+        xo, so = ref.solve(pr["xu"].astype(np.float64), 0.01, pr["xs"], pr["goal"])
+        st = mx.stats(c)
+        np.testing.assert_array_equal(st["pcg_iters"], so["pcg_iters"])
+        np.testing.assert_array_equal(st["ls_step_size"], so["ls_step_size"].astype(np.float32))
+        np.testing.assert_array_equal(st["status"], so["status"])
+        assert nerr(xu[c].cpu().numpy(), xo) < 1e-8, (plant, N)
     mx.close()

@@ -171,3 +171,45 @@ def test_rollout_autograd_reaches_the_weights():
         assert t.grad is not None and torch.isfinite(t.grad).all()
     assert float(logr.grad.abs().sum()) > 0
     s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_hypothesis_selection_matches_oracle_simulator(oracle_mod, precision):
+    """Batch-hypothesis selection (gato_select_hypothesis,
+    mpc_controller.py:295-309): each problem's one-step simulation under its
+    own wrench hypothesis is scored against a measured state made by the
+    oracle's simulator under hypothesis 5; errors match the oracle's, the
+    argmin is 5, and the winner's trajectory is broadcast to every row."""
+    import torch
+    import gato_b200
+    from gato_b200 import mpc
+    torch.cuda.set_device(0)
+    O = oracle_mod
+    plant, Bh, Nh, dt = "iiwa14", 16, 8, 0.01
+    rng = np.random.default_rng(67)
+    s = gato_b200.BSQP(batch_size=Bh, N=Nh, dt=dt, plant_type=plant, precision=precision)
+    f = rng.normal(0, 5, (Bh, 6))
+    s.set_f_ext_B(f)
+    x_last = np.concatenate([rng.uniform(-1, 1, 7), rng.normal(0, 0.3, 7)])
+    u_last = rng.normal(0, 5, 7)
+    m = O.Model(plant)
+
+    def sim(b):
+        qdd = m.fd(x_last[:7], x_last[7:], u_last, f[b].astype(np.float32).astype(np.float64))
+        return np.concatenate([x_last[:7] + dt * x_last[7:] + 0.5 * qdd * dt * dt,
+                               x_last[7:] + dt * qdd])
+
+    x_curr = sim(5) + rng.normal(0, 1e-7, 14)
+    ref_err = np.array([np.linalg.norm(sim(b) - x_curr) for b in range(Bh)])
+    dtt = torch.float64 if precision == "fp64" else torch.float32
+    T = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=dtt, device="cuda")
+    xu = T(rng.normal(0, 1, (Bh, s.traj_size)))
+    row5 = xu[5].clone()
+    x_l, u_l, x_c = T(x_last), T(u_last), T(x_curr)
+    best, err = mpc.select_hypothesis(s, x_l, u_l, x_c, dt, xu=xu)
+    torch.cuda.synchronize()
+    s.close()
+    assert best == 5
+    tol = 1e-12 if precision == "fp64" else 2e-5
+    np.testing.assert_allclose(err.double().cpu().numpy(), ref_err, rtol=0, atol=tol)
+    assert torch.equal(xu, row5.expand(Bh, -1))
