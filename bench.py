@@ -68,7 +68,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=1024)
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "fp64"],
+                    help="headline solver arithmetic (fp64: profile workload only)")
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="problems in the CPU baseline sample (0: sized to ~10 s)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
@@ -498,23 +499,45 @@ def time_device_steps(torch, solver, bufs, wl, steps, warmup, flush, stream):
 PRECISIONS = ("fp32", "mixed", "fp64")
 
 
+def profile_kernels(solver, wl, bufs, stream):
+    """Device time per kernel group of one solve from the warm start
+    (gato_profile_solve: CUDA events around every launch, the fused form
+    without its graph): {group: {"ms", "launches"}}."""
+    import ctypes
+    import gato_b200._lib as L
+    d_xu, d_xs, d_goal, d_xu0 = bufs
+    d_xu.copy_(d_xu0)
+    solver.set_lambda(wl["lam"])
+    solver.reset_rho()
+    msk = (ctypes.c_double * len(L.KERNELS))()
+    nk = (ctypes.c_int32 * len(L.KERNELS))()
+    fn = L.load().gato_profile_solve_f64 if solver.precision == "fp64" else \
+        L.load().gato_profile_solve
+    L.check(fn(solver._h, ctypes.c_void_p(stream.cuda_stream), L.vptr(d_xu), L.vptr(d_xs),
+               L.vptr(d_goal), msk, nk))
+    return {L.KERNELS[i]: {"ms": msk[i], "launches": nk[i]} for i in range(len(L.KERNELS))}
+
+
 def precision_times(torch, dev, B, prec, wl, args, flush, stream):
     """Mean ms per solve of the fused and the plain form in precision
-    `prec` on the workload (inputs resident, timed like the headline)."""
+    `prec` on the workload (inputs resident, timed like the headline), and
+    each form's device time per kernel group ({"fused": ..., "plain": ...})."""
     import gato_b200
     dt = torch.float64 if prec == "fp64" else torch.float32
     T = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
     d_xu0, d_xs, d_goal = T(wl["xu"]), T(wl["xs"]), T(wl["goal"])
     bufs = (d_xu0.clone(), d_xs, d_goal, d_xu0)
     out = []
+    kern = {}
     for form in ("fused", "plain"):
         s = gato_b200.BSQP(batch_size=B, N=N, dt=DT, plant_type=PLANT, form=form,
                            precision=prec, **solver_kwargs())
         steps = args.steps if form == "fused" else max(3, args.steps // 2)
         out.append(float(np.mean(time_device_steps(torch, s, bufs, wl, steps, max(1, args.warmup),
                                                    flush, stream))))
+        kern[form] = profile_kernels(s, wl, bufs, stream)
         s.close()
-    return out
+    return out[0], out[1], kern
 
 
 def trajectory_errors(xg, xo):
@@ -705,15 +728,20 @@ def adjoint_config4(torch, dev, threads, precisions=PRECISIONS, B=ADJ_B, fd_prob
                                  for k, v in errs.items()}}
         res["backward_vs_forward"] = res["adjoint_ms"] / res["forward_ms"]
         if prec == "fp64" and fd_problems:
-            res["fd_device_vs_dense"] = _device_fd(torch, dev, s, xu, wl, w_held, rho, lam, dln,
-                                                   dense, fd_problems)
+            # h = 1e-6 as specified; its error is rounding noise of the QP
+            # solve divided by h (cond(KKT) ~ 1e5-1e6 here), so h = 1e-4, whose
+            # truncation error is below that noise, is reported beside it
+            res["fd_device_vs_dense"] = _device_fd(torch, dev, xu, wl, w_held, rho, lam, dln,
+                                                   dense, fd_problems, ADJ_H)
+            res["fd_device_vs_dense_h1e-4"] = _device_fd(torch, dev, xu, wl, w_held, rho, lam,
+                                                         dln, dense, fd_problems, 1e-4)
         s.close()
         out[prec] = res
     return out
 
 
-def _device_fd(torch, dev, s, xu, wl, w_held, rho, lam, dl, dense, K):
-    """Central differences (h = ADJ_H, on x0, the goal positions and the log
+def _device_fd(torch, dev, xu, wl, w_held, rho, lam, dl, dense, K, h):
+    """Central differences (step h, on x0, the goal positions and the log
     weights) of l(theta) = dl . (xu + dz(theta)), dz the QP step at the fixed
     xu computed by the device in FP64 (gato_qp_step_f64, 1500 PCG iterations
     for every evaluation, no tolerance stop), for the first K problems: all
@@ -737,16 +765,15 @@ def _device_fd(torch, dev, s, xu, wl, w_held, rho, lam, dl, dense, K):
     for r, (b, kind, i, sgn) in enumerate(rows):
         xs[r], goal[r], wd[r], xum[r] = wl["xs"][b], wl["goal"][b], w_held[b], xu[b]
         if kind == "x0":
-            xs[r, i] += sgn * ADJ_H
+            xs[r, i] += sgn * h
         elif kind == "goal":
-            goal[r, i] += sgn * ADJ_H
+            goal[r, i] += sgn * h
         else:
-            wd[r, i] *= np.exp(sgn * ADJ_H)
+            wd[r, i] *= np.exp(sgn * h)
     f = gato_b200.BSQP(batch_size=M, N=N, dt=DT, plant_type=PLANT, precision="fp64",
                        **solver_kwargs())
     f.set_cost_diag_batch(wd[:, :nx], wd[:, nx:])
-    f.set_rho_penalty_batch(np.array([rho[b] for b, *_ in rows]), False)
-    f.reset_rho()
+    f.set_rho_penalty_batch(np.array([rho[b] for b, *_ in rows]), True)
     f.set_lambda(np.stack([lam[b] for b, *_ in rows]))
     T = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
     d_xu, d_xs, d_goal = T(xum), T(xs), T(goal)
@@ -762,18 +789,21 @@ def _device_fd(torch, dev, s, xu, wl, w_held, rho, lam, dl, dense, K):
     for b in range(K):
         fd = {"x0": [], "goal": [], "w": []}
         for kind, i in params:
-            fd[kind].append((loss[r] - loss[r + 1]) / (2 * ADJ_H))
+            fd[kind].append((loss[r] - loss[r + 1]) / (2 * h))
             r += 2
         d = dense[b]
         errs["x0"].append(_rel_err(fd["x0"], d["g_xs"]))
         errs["goal"].append(_rel_err(fd["goal"], d["g_goal"][gi]))
         errs["log_qr"].append(_rel_err(fd["w"], d["g_wdiag"] * w_held[b]))
-    return {"problems": K, "h": ADJ_H, "pcg_iters": 1500,
+    return {"problems": K, "h": h, "pcg_iters": 1500,
             "rel_err": {k: {"median": float(np.median(v)), "max": float(np.max(v))}
                         for k, v in errs.items()}}
 
 
 def run_ours(args):
+    if args.precision == "fp64":
+        raise SystemExit("--precision fp64 applies to --workload profile only (the headline "
+                         "line reports FP64 under by_precision)")
     import torch
     import gato_b200
     import gato_b200._lib as L
@@ -810,15 +840,7 @@ def run_ours(args):
     st = fused.solve_device(d_xu, d_xs, d_goal, stream=stream.cuda_stream)
     pcg_total = int(np.sum(st["pcg_iters"]))
     # per-kernel device times of the same solve (events around each launch)
-    d_xu.copy_(d_xu0)
-    fused.set_lambda(wl["lam"])
-    fused.reset_rho()
-    import ctypes
-    msk = (ctypes.c_double * len(L.KERNELS))()
-    nk = (ctypes.c_int32 * len(L.KERNELS))()
-    L.check(L.load().gato_profile_solve(fused._h, ctypes.c_void_p(stream.cuda_stream),
-                                        L.vptr(d_xu), L.vptr(d_xs), L.vptr(d_goal), msk, nk))
-    kern = {L.KERNELS[i]: {"ms": msk[i], "launches": nk[i]} for i in range(len(L.KERNELS))}
+    kern = profile_kernels(fused, wl, bufs, stream)
     total_prof = sum(v["ms"] for v in kern.values())
 
     peaks = measured_peaks()
@@ -892,14 +914,25 @@ def run_ours(args):
     by_prec = {args.precision: {"value": B / (float(np.mean(t_fused)) * 1e-3),
                                 "plain_value": B / (float(np.mean(t_plain)) * 1e-3),
                                 "fused_vs_plain": float(np.mean(t_plain) / np.mean(t_fused))}}
+    kern_by_prec = {args.precision: {k: round(v["ms"], 4) for k, v in kern.items()
+                                     if v["launches"]}}
+    plain_kern_by_prec = {args.precision: None}
     for prec in PRECISIONS:
         if prec in by_prec:
             continue
-        tf, tp = precision_times(torch, dev, B, prec, wl, args, flush, stream)
+        tf, tp, kp = precision_times(torch, dev, B, prec, wl, args, flush, stream)
         by_prec[prec] = {"value": B / (tf * 1e-3), "plain_value": B / (tp * 1e-3),
                          "fused_vs_plain": tp / tf}
+        kern_by_prec[prec] = {k: round(v["ms"], 4) for k, v in kp["fused"].items()
+                              if v["launches"]}
+        plain_kern_by_prec[prec] = {k: round(v["ms"], 4) for k, v in kp["plain"].items()
+                                    if v["launches"]}
     by_prec = {k: {kk: max_over_ranks(vv, dist, dev) for kk, vv in v.items()}
                for k, v in by_prec.items()}
+    for k in by_prec:
+        by_prec[k]["kernels_ms"] = kern_by_prec[k]
+        if plain_kern_by_prec.get(k):
+            by_prec[k]["plain_kernels_ms"] = plain_kern_by_prec[k]
 
     # CPU baseline (rank 0, N=1 only)
     cpu = None
@@ -1315,7 +1348,9 @@ def run_profile(args):
     xu[:, :2 * nq] = pr["xs"]
     kw = dict(max_sqp_iters=args.sqp_iters, pcg_tol=PCG_TOL, max_pcg_iters=PCG_MAX)
     dev = torch.device("cuda")
-    T = lambda x: torch.tensor(np.ascontiguousarray(x), dtype=torch.float32, device=dev)
+    f64 = args.precision == "fp64"
+    dt_ = torch.float64 if f64 else torch.float32
+    T = lambda x: torch.tensor(np.ascontiguousarray(x), dtype=dt_, device=dev)
     d_xs, d_goal = T(pr["xs"]), T(pr["goal"])
     for form in ("plain", "fused"):
         s = gato_b200.BSQP(batch_size=args.batch, N=args.horizon, dt=DT, plant_type=args.plant,
@@ -1323,8 +1358,8 @@ def run_profile(args):
         d_xu = T(xu)
         ms = (ctypes.c_double * len(L.KERNELS))()
         n = (ctypes.c_int32 * len(L.KERNELS))()
-        L.check(L.load().gato_profile_solve(s._h, None, L.vptr(d_xu), L.vptr(d_xs),
-                                            L.vptr(d_goal), ms, n))
+        fn = L.load().gato_profile_solve_f64 if f64 else L.load().gato_profile_solve
+        L.check(fn(s._h, None, L.vptr(d_xu), L.vptr(d_xs), L.vptr(d_goal), ms, n))
         print(form, {L.KERNELS[i]: round(ms[i], 3) for i in range(len(L.KERNELS)) if n[i]})
         s.close()
     return 0

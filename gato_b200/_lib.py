@@ -116,10 +116,13 @@ SIGNATURES = {
     "gato_sim_forward": (ctypes.c_int, [_vp, _fp, _fp, ctypes.c_float, _fp]),
     "gato_profile_solve": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp,
                                           ctypes.POINTER(ctypes.c_double), _ip]),
+    "gato_profile_solve_f64": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp,
+                                              ctypes.POINTER(ctypes.c_double), _ip]),
     "gato_stage_setup_kkt": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp] + [_vp] * 7),
     "gato_stage_form_schur": (ctypes.c_int, [_vp, _vp] + [_vp] * 10),
     "gato_stage_pcg": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gato_set_cost_diag_batch": (ctypes.c_int, [_vp, _vp]),
+    "gato_set_cost_diag_batch_f64": (ctypes.c_int, [_vp, _vp]),
     "gato_rollout": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gato_rollout_backward": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp,
                                              _vp, _vp, _vp, _vp, ctypes.c_double,

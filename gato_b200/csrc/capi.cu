@@ -198,11 +198,9 @@ int gato_solve_host_f64(gato_solver_t* s, double* h_xu, double dt, const double*
     return solve_host_any(s, h_xu, dt, h_xs, h_goal, stats);
 }
 
-int gato_profile_solve(gato_solver_t* s, void* stream, float* d_xu, const float* d_xs,
-                       const float* d_goal, double* ms_by_kernel, int32_t* launches_by_kernel)
+static int profile_any(gato_solver_t* s, void* stream, void* d_xu, const void* d_xs,
+                       const void* d_goal, double* ms_by_kernel, int32_t* launches_by_kernel)
 {
-    RC(check_handle(s));
-    RC(check_single(s));
     if (!d_xu || !d_xs || !d_goal || !ms_by_kernel || !launches_by_kernel)
         return fail(GATO_ERR_ARG, "null pointer");
     RC(bind_device(s));
@@ -238,6 +236,23 @@ int gato_profile_solve(gato_solver_t* s, void* stream, float* d_xu, const float*
     return check_device_waits(s);
 }
 
+int gato_profile_solve(gato_solver_t* s, void* stream, float* d_xu, const float* d_xs,
+                       const float* d_goal, double* ms_by_kernel, int32_t* launches_by_kernel)
+{
+    RC(check_handle(s));
+    RC(check_single(s));
+    return profile_any(s, stream, d_xu, d_xs, d_goal, ms_by_kernel, launches_by_kernel);
+}
+
+int gato_profile_solve_f64(gato_solver_t* s, void* stream, double* d_xu, const double* d_xs,
+                           const double* d_goal, double* ms_by_kernel,
+                           int32_t* launches_by_kernel)
+{
+    RC(check_handle(s));
+    RC(check_double(s));
+    return profile_any(s, stream, d_xu, d_xs, d_goal, ms_by_kernel, launches_by_kernel);
+}
+
 int gato_set_wait_limits(gato_solver_t* s, int copy_tries, int step_copy_tries)
 {
     RC(check_handle(s));
@@ -263,24 +278,40 @@ int gato_set_f_ext_batch(gato_solver_t* s, const float* h_f_ext)
     return GATO_OK;
 }
 
-int gato_set_cost_diag_batch(gato_solver_t* s, const float* h_wdiag)
+// v: the weights widened to double, or null to return to the scalar weights
+static int set_cost_diag(gato_solver_t* s, const std::vector<double>* v)
 {
     RC(check_handle(s));
     RC(bind_device(s));
-    const int use = h_wdiag != nullptr;
+    const int use = v != nullptr;
     if (use) {
         const size_t n = (size_t)3 * s->nq * s->B;
-        std::vector<double> v(h_wdiag, h_wdiag + n);
-        for (double x : v)
+        for (double x : *v)
             if (!std::isfinite(x)) return fail(GATO_ERR_ARG, "non-finite cost weight");
         if (!s->wdiag) RC(s->alloc_t(&s->wdiag, n));
-        RC(s->upload(s->wdiag, v.data(), n));
+        RC(s->upload(s->wdiag, v->data(), n));
     }
     if (use != s->use_wdiag) {
         s->use_wdiag = use;
         s->version++;
     }
     return GATO_OK;
+}
+
+int gato_set_cost_diag_batch(gato_solver_t* s, const float* h_wdiag)
+{
+    RC(check_handle(s));
+    if (!h_wdiag) return set_cost_diag(s, nullptr);
+    std::vector<double> v(h_wdiag, h_wdiag + (size_t)3 * s->nq * s->B);
+    return set_cost_diag(s, &v);
+}
+
+int gato_set_cost_diag_batch_f64(gato_solver_t* s, const double* h_wdiag)
+{
+    RC(check_handle(s));
+    if (!h_wdiag) return set_cost_diag(s, nullptr);
+    std::vector<double> v(h_wdiag, h_wdiag + (size_t)3 * s->nq * s->B);
+    return set_cost_diag(s, &v);
 }
 
 int gato_set_rho_penalty_batch(gato_solver_t* s, const float* h_rho, int set_as_reset_default)

@@ -454,7 +454,9 @@ __device__ int pcg_block(int N, const T* __restrict__ S, const T* __restrict__ P
         part = btd_mv<NQ, T, Acc>(N, P, r, z, r);
         const Acc rho_new = block_sum<Acc>(part, red + WARP);
         const Acc arn = rho_new < 0 ? -rho_new : rho_new;
-        if (arn < abs_tol + (Acc)eps * rho_init || !(arn > 0)) break;
+        // the reference's stop (pcg.cuh:128-129); an exact zero also stops (reachable
+        // only with a zero tolerance), a NaN runs on to the cap as it does there
+        if (arn < abs_tol + (Acc)eps * rho_init || arn == 0) break;
         const Acc beta = rho_new / rho;
         rho = rho_new;
         const T bf = (T)beta;
@@ -545,6 +547,9 @@ __host__ __device__ constexpr int pcg_rows_per_thread()
     return sizeof(T) == 4 ? 2 : 1;
 }
 
+template <int NQ>
+struct SmemRows;
+
 template <int NQ, int RPT>
 struct RowPcg {
     static constexpr int n = 2 * NQ, m = NQ, RD = 3 * n, VS = row_vs(n);
@@ -557,6 +562,15 @@ struct RowPcg {
     __host__ __device__ static size_t smem_bytes(int N)
     {
         return 2 * (size_t)(N + 2) * VS * sizeof(T) + 2 * WARP * sizeof(double) + 16;
+    }
+    // FP64 with P^-1 in shared memory (k_pcg_rows_psm): one row per thread,
+    // at most PSM_THREADS threads (registers for S: 65536 / 448 = 146 a thread)
+    static constexpr int PSM_THREADS = 448;
+    __host__ __device__ static bool fits_psm(int N) { return RPT == 1 && N * TPB <= PSM_THREADS; }
+    __host__ __device__ static size_t smem_bytes_psm(int N)
+    {
+        return smem_bytes<double>(N) + 16 +
+               (size_t)RD * SmemRows<NQ>::stride(threads(N)) * sizeof(double);
     }
 };
 
@@ -655,6 +669,55 @@ __device__ __forceinline__ void rows_window_dot(const RowMat<NQ, RPT, float>& ro
                  ((acc[j][2].x + acc[j][2].y) + (acc[j][3].x + acc[j][3].y));
 }
 
+// FP64 P^-1 rows in shared memory, one row per thread.  An FP64 problem's S
+// and P^-1 (2 x 150 KB for iiwa14 N = 32) do not fit in one SM's registers
+// together: S stays in registers and P^-1 is stored transposed, entry (row r,
+// column c) of the [N n][3n] block-row layout at pt[c * rs + r], rs = the
+// CTA's thread count + 1 (odd).  A warp's load of one column then reads 32
+// consecutive doubles (two wavefronts, no conflicts), and the cooperative
+// fill, which walks the global rows in order, spreads its stores over the
+// banks.  The dot product keeps the register form's four partial sums by
+// column mod 4, so the iterates are those of k_pcg_rows bit for bit.
+template <int NQ>
+struct SmemRows {
+    static constexpr int n = 2 * NQ, RD = 3 * n;
+    double* pt;
+    int rs, row;
+    // every thread of the CTA: rows [0, nrows) of src into pt, zero rows up
+    // to the thread count; a barrier must follow before the first dot
+    __device__ __forceinline__ void fill(const double* __restrict__ src, int nrows) const
+    {
+        const int total = nrows * RD;
+        for (int e = threadIdx.x; e < total; e += blockDim.x) {
+            const int r = e / RD, c = e - r * RD;
+            pt[c * rs + r] = src[e];
+        }
+        for (int r = nrows + threadIdx.x; r < (int)blockDim.x; r += blockDim.x)
+#pragma unroll
+            for (int c = 0; c < RD; ++c) pt[c * rs + r] = 0.0;
+    }
+    __host__ __device__ static int stride(int threads) { return threads + 1; }
+};
+
+template <int NQ>
+__device__ __forceinline__ void rows_window_dot(const SmemRows<NQ>& p, const double* win,
+                                                double (&out)[1])
+{
+    constexpr int n = 2 * NQ, VS = row_vs(n);
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const double* col = p.pt + p.row;
+#pragma unroll
+    for (int blk = 0; blk < 3; ++blk) {
+#pragma unroll
+        for (int c0 = 0; c0 < n; c0 += 2) {
+            const double2 v = *reinterpret_cast<const double2*>(win + blk * VS + c0);
+            acc[c0 & 3] += col[(blk * n + c0) * p.rs] * v.x;
+            acc[(c0 + 1) & 3] += col[(blk * n + c0 + 1) * p.rs] * v.y;
+        }
+    }
+    out[0] = (acc[0] + acc[1]) + (acc[2] + acc[3]);
+}
+
 template <typename Acc>
 __device__ __forceinline__ Acc rows_block_sum(Acc v, Acc* red)
 {
@@ -706,7 +769,7 @@ struct NoDzStage {
 // threads where dz_ready() returns true (each thread decides for itself; no
 // barrier depends on it), else read from global memory.
 template <int NQ, typename T, typename Acc, int RPT, class Hook = NoHook,
-          class DzReady = NoDzStage>
+          class DzReady = NoDzStage, bool PSM = false>
 __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int it_row,
                                               unsigned char* smem_raw, const T* Sp = nullptr,
                                               const T* Pp = nullptr, Hook hook = Hook(),
@@ -734,12 +797,23 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
 #pragma unroll
     for (int j = 0; j < RPT; ++j) x[j] = act ? lam[(k + 1) * n + i0 + j * TPB] : T(0);
     if (!bt.conv[b]) {
-        RowMat<NQ, RPT, T> srow, prow;
+        // PSM: P^-1 in shared memory after the reduction slots (FP64, RPT = 1)
+        static_assert(!PSM || (RPT == 1 && sizeof(T) == 8), "P^-1 in shared memory is FP64");
+        RowMat<NQ, RPT, T> srow;
+        std::conditional_t<PSM, SmemRows<NQ>, RowMat<NQ, RPT, T>> prow;
         {
             const size_t row = (size_t)(k * n + i0) * RD;
             const size_t prob = (size_t)b * d.b3d();
             srow.load((Sp ? Sp : bt.S + prob) + row, (size_t)TPB * RD, act);
-            prow.load((Pp ? Pp : bt.P + prob) + row, (size_t)TPB * RD, act);
+            if constexpr (PSM) {
+                prow.pt = reinterpret_cast<double*>(
+                    ((uintptr_t)(red + 2 * WARP) + 15) & ~(uintptr_t)15);
+                prow.rs = SmemRows<NQ>::stride(blockDim.x);
+                prow.row = tid;
+                prow.fill(reinterpret_cast<const double*>(Pp ? Pp : bt.P + prob), N * n);
+            } else {
+                prow.load((Pp ? Pp : bt.P + prob) + row, (size_t)TPB * RD, act);
+            }
         }
         T g[RPT], r[RPT], z[RPT], p[RPT], ap[RPT];
 #pragma unroll
@@ -785,7 +859,9 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
             if (!(fabs((double)rho) < (double)abs_tol)) {
                 const Acc rho_init = rho < 0 ? -rho : rho;
                 Acc alpha = rho / delta;
-                const bool start = isfinite((double)alpha);  // delta = 0: nothing to do
+                // delta = 0: nothing to do; a NaN runs on (and stops at the
+                // breakdown test), so the problem is not taken as converged
+                const bool start = !(delta == 0);
 #pragma unroll
                 for (int j = 0; j < RPT; ++j) {
                     p[j] = z[j];
@@ -858,7 +934,7 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
 #pragma unroll
                     for (int j = 0; j < RPT; ++j) part += act ? (Acc)p[j] * (Acc)ap[j] : Acc(0);
                     const Acc pap = rows_block_sum<Acc>(part, red);
-                    if (!(fabs((double)pap) > 0) || !isfinite((double)pap)) break;
+                    if (pap == 0) break;
                     const T alpha = (T)(rho / pap);
 #pragma unroll
                     for (int j = 0; j < RPT; ++j) {
@@ -873,7 +949,7 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
                     for (int j = 0; j < RPT; ++j) part += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);
                     const Acc rho_new = rows_block_sum<Acc>(part, red + WARP);
                     const Acc arn = rho_new < 0 ? -rho_new : rho_new;
-                    if (arn < abs_tol + (Acc)eps * rho_init || !(arn > 0)) break;
+                    if (arn < abs_tol + (Acc)eps * rho_init || arn == 0) break;
                     const T beta = (T)(rho_new / rho);
                     rho = rho_new;
 #pragma unroll
@@ -970,6 +1046,18 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     pcg_rows_body<NQ, T, Acc, RPT>(bt, blockIdx.x, it_row, smem_raw);
+}
+
+// FP64 k_pcg_rows with S in registers and P^-1 in shared memory (one row per
+// thread; the register form of FP64 holds both and spills).  Same iterates.
+// (at most PSM_THREADS = 448 threads: 14 warps, four on one of the SM's four
+// 16K-register partitions, so 128 registers a thread)
+template <int NQ, typename Acc>
+__global__ void __launch_bounds__(RowPcg<NQ, 1>::PSM_THREADS, 1)
+    k_pcg_rows_psm(Batch<NQ, double> bt, int it_row)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    pcg_rows_body<NQ, double, Acc, 1, NoHook, NoDzStage, true>(bt, blockIdx.x, it_row, smem_raw);
 }
 
 // Persistent FP32 form of k_pcg_rows: one CTA per SM takes problems from a

@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
             if (!(fabs((double)rho) < (double)abs_tol)) {
                 const Acc rho_init = rho < 0 ? -rho : rho;
                 Acc alpha = rho / delta;
-                const bool start = isfinite((double)alpha);  // delta = 0: nothing to do
+                const bool start = !(delta == 0);  // delta = 0: nothing to do
 #pragma unroll
                 for (int j = 0; j < RPT; ++j) {
                     p[j] = z[j];
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
 #pragma unroll
                     for (int j = 0; j < RPT; ++j) pap += act ? (Acc)p[j] * (Acc)w[j] : Acc(0);
                     csum2(pap, unused);
-                    if (!(fabs((double)pap) > 0) || !isfinite((double)pap)) break;
+                    if (pap == 0) break;
                     const T alpha = (T)(rho / pap);
 #pragma unroll
                     for (int j = 0; j < RPT; ++j) {
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
                     for (int j = 0; j < RPT; ++j) rho_new += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);
                     csum2(rho_new, unused);
                     const Acc arn = rho_new < 0 ? -rho_new : rho_new;
-                    if (arn < abs_tol + (Acc)eps * rho_init || !(arn > 0)) break;
+                    if (arn < abs_tol + (Acc)eps * rho_init || arn == 0) break;
                     const T beta = (T)(rho_new / rho);
                     rho = rho_new;
 #pragma unroll

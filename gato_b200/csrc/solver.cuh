@@ -508,6 +508,18 @@ bool pcg_stream_dz_fits(const gato_solver* s)
         return false;
 }
 
+// FP64 runs k_pcg_rows_psm (S in registers, P^-1 in shared memory) where
+// one row per thread fits its thread limit and P^-1 fits shared memory
+template <class Tg>
+bool pcg_psm_fits(const gato_solver* s)
+{
+    if constexpr (sizeof(typename Tg::T) == 8)
+        return RowPcg<Tg::NQ, 1>::fits_psm(s->N) &&
+               RowPcg<Tg::NQ, 1>::smem_bytes_psm(s->N) <= (size_t)s->max_smem;
+    else
+        return false;
+}
+
 // register-resident PCG + dz of every problem
 template <class Tg>
 void launch_pcg_rows(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt,
@@ -524,6 +536,13 @@ void launch_pcg_rows(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typena
                                          dz ? PcgStage<NQ>::smem_bytes_dz(s->N)
                                             : PcgStage<NQ>::smem_bytes(s->N),
                                          st>>>(bt, row, dz);
+            return;
+        }
+    }
+    if constexpr (sizeof(T) == 8) {
+        if (pcg_psm_fits<Tg>(s)) {
+            k_pcg_rows_psm<NQ, Acc><<<s->B, RowPcg<NQ, 1>::threads(s->N),
+                                      RowPcg<NQ, 1>::smem_bytes_psm(s->N), st>>>(bt, row);
             return;
         }
     }
@@ -655,6 +674,11 @@ int configure_kernels(gato_solver* s)
     constexpr int RPT = pcg_rows_per_thread<T>();
     RC(set_smem(k_pcg_rows<NQ, T, Acc, RPT>, RowPcg<NQ, RPT>::template smem_bytes<T>(s->N),
                 s->max_smem));
+    if constexpr (sizeof(T) == 8) {
+        if (pcg_psm_fits<Tg>(s))
+            RC(set_smem(k_pcg_rows_psm<NQ, Acc>, RowPcg<NQ, 1>::smem_bytes_psm(s->N),
+                        s->max_smem));
+    }
     if constexpr (sizeof(T) == 4) {
         if (pcg_stream_fits<Tg>(s))
             RC(set_smem(k_pcg_rows_stream<NQ, Acc>,

@@ -302,17 +302,22 @@ class BSQP:
         """Per-problem diagonal weights: q_diag [B, nx] on the state, r_diag
         [B, nu] on the control (the stage cost gains 1/2 Qd_i x_i^2 and
         1/2 Rd_i u_i^2 in place of the scalar qd_cost and u_cost terms).
-        Both None returns to the scalar weights.  No counterpart in the
+        Both None returns to the scalar weights.  FP64 solvers keep them in
+        FP64, the others round them to float.  No counterpart in the
         reference; these are the Q/R diagonals the adjoint differentiates."""
         if q_diag is None and r_diag is None:
             self._wdiag = None
             L.check(L.load().gato_set_cost_diag_batch(self._h, None))
             return
         B = self.batch_size
-        qd = np.broadcast_to(np.asarray(q_diag, np.float32), (B, self.nx))
-        rd = np.broadcast_to(np.asarray(r_diag, np.float32), (B, self.nu))
-        self._wdiag = np.ascontiguousarray(np.concatenate([qd, rd], axis=1), dtype=np.float32)
-        L.check(L.load().gato_set_cost_diag_batch(self._h, L.fptr(self._wdiag)))
+        f = np.float64 if self.precision == "fp64" else np.float32
+        qd = np.broadcast_to(np.asarray(q_diag, f), (B, self.nx))
+        rd = np.broadcast_to(np.asarray(r_diag, f), (B, self.nu))
+        self._wdiag = np.ascontiguousarray(np.concatenate([qd, rd], axis=1), dtype=f)
+        if f is np.float64:
+            L.check(L.load().gato_set_cost_diag_batch_f64(self._h, L.dptr(self._wdiag)))
+        else:
+            L.check(L.load().gato_set_cost_diag_batch(self._h, L.fptr(self._wdiag)))
 
     def default_cost_diag(self):
         """(q_diag, r_diag) equal to the scalar weights: [0, qd_cost] and

@@ -221,6 +221,10 @@ enum {
    The reference only times the whole solve on the host (bsqp.cuh:109-190). */
 int gato_profile_solve(gato_solver_t* s, void* stream, float* d_xu, const float* d_xs,
                        const float* d_goal, double* ms_by_kernel, int32_t* launches_by_kernel);
+/* The same for FP64 solvers (double buffers). */
+int gato_profile_solve_f64(gato_solver_t* s, void* stream, double* d_xu, const double* d_xs,
+                           const double* d_goal, double* ms_by_kernel,
+                           int32_t* launches_by_kernel);
 
 /* Per-problem diagonal cost weights (no counterpart in the reference, whose
    weights are the scalars qd_cost and u_cost): h_wdiag [B][nx+nu] =
@@ -230,6 +234,9 @@ int gato_profile_solve(gato_solver_t* s, void* stream, float* d_xu, const float*
    cost.  NULL returns to the scalar weights.  These are the Q/R diagonals
    that gato_adjoint differentiates. */
 int gato_set_cost_diag_batch(gato_solver_t* s, const float* h_wdiag);
+/* The same with FP64 weights, kept at full precision by FP64 solvers (FP32
+   and mixed solvers round them to float). */
+int gato_set_cost_diag_batch_f64(gato_solver_t* s, const double* h_wdiag);
 /* Batched setters (host arrays of B floats, or 6*B for f_ext; FP64 solvers
    widen them).
    Replace BSQP::set_f_ext_batch / set_rho_penalty_batch / set_drho_batch /

@@ -1057,7 +1057,10 @@ enum {
     ORC_ROUND_KKT = 1,    /* Q, R, q, r, A, B, c after the KKT set-up */
     ORC_ROUND_SCHUR = 2,  /* S, P^-1, gamma, (Q+rho I)^-1, R^-1 */
     ORC_ROUND_LAMBDA = 4, /* lambda after the PCG */
-    ORC_ROUND_XU = 8      /* XU after the line-search update */
+    ORC_ROUND_XU = 8,     /* XU after the line-search update */
+    ORC_ROUND_S = 16,     /* S alone */
+    ORC_ROUND_PINV = 32,  /* P^-1 alone */
+    ORC_ROUND_GAMMA = 64  /* gamma alone */
 };
 static void round_f32(double* p, size_t n)
 {
@@ -1131,6 +1134,9 @@ static void solve(Solver& S, double dt, double* xu, const double* xs, const doub
                 round_f32(Qb, (size_t)N * nx * nx);
                 round_f32(Rb, (size_t)N * nu * nu);
             }
+            if (S.round_f32 & ORC_ROUND_S) round_f32(&Sm[b * d.b3d()], d.b3d());
+            if (S.round_f32 & ORC_ROUND_PINV) round_f32(&Pi[b * d.b3d()], d.b3d());
+            if (S.round_f32 & ORC_ROUND_GAMMA) round_f32(&gam[b * L], L);
             pcg_it[b] = conv[b] ? 0
                                 : pcg(d, &Sm[b * d.b3d()], &Pi[b * d.b3d()], &gam[b * L],
                                       &S.lambda[b * L], S.tol[b], P.max_pcg_iters);

@@ -94,7 +94,7 @@ def test_fp64_mixed_solve_reproduces_oracle(oracle_mod):
     """One FP64 mixed solve over four classes, the N = 128 class (cluster
     PCG on a parallel graph branch) among them: every class reproduces the
     FP64 oracle run on the same problems (iteration counts, line-search
-    steps, trajectories to 1e-8)."""
+    steps, status, trajectories to 1e-8; 1e-5 for the cluster class)."""
     import torch
     from gato_b200.mixed import MixedBSQP
     torch.cuda.set_device(0)
@@ -113,5 +113,14 @@ def test_fp64_mixed_solve_reproduces_oracle(oracle_mod):
         np.testing.assert_array_equal(st["pcg_iters"], so["pcg_iters"])
         np.testing.assert_array_equal(st["ls_step_size"], so["ls_step_size"].astype(np.float32))
         np.testing.assert_array_equal(st["status"], so["status"])
-        assert nerr(xu[c].cpu().numpy(), xo) < 1e-8, (plant, N)
+        # the N = 128 class sums its PCG inner products per CTA of the
+        # cluster, then across CTAs: with equal iteration counts and steps,
+        # that summation order alone moves its trajectories by ~1e-6, and the
+        # class solved alone by the fused form (the same cluster PCG) gives
+        # the mixed solve's result bit for bit
+        assert nerr(xu[c].cpu().numpy(), xo) < (1e-5 if N > 64 else 1e-8), (plant, N)
+        if N > 64:
+            xa, pa, _ = _alone(plant, N, B, pr, "fp64", T)
+            np.testing.assert_array_equal(xa, xu[c].cpu().numpy())
+            np.testing.assert_array_equal(pa, st["pcg_iters"])
     mx.close()
