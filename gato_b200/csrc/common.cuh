@@ -162,5 +162,11 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
+// ends an mbarrier's life (before its memory is initialised again); every
+// phase it tracked must have completed
+__device__ __forceinline__ void mbar_inval(uint64_t* bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
 
 }  // namespace gato

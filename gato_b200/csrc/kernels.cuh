@@ -15,7 +15,14 @@
 #include "dynamics_thread.cuh"
 #include "stages.cuh"
 
+
 namespace gato {
+
+// bounds (mbarrier try_wait calls of about 1 us each) of the waits for bulk
+// copies into shared memory: the default wait, and the drain of a copy whose
+// wait expired before the CTA stops using its buffer
+constexpr int PCG_STAGE_WAIT_TRIES = 1 << 22;
+constexpr int PCG_STAGE_DRAIN_TRIES = 1 << 22;
 
 // Per-solver device state handed to every kernel by value.
 template <int NQ, typename T>
@@ -544,10 +551,23 @@ __host__ __device__ constexpr int row_vs(int n)
 template <typename T>
 __host__ __device__ constexpr int pcg_rows_per_thread()
 {
+    return 2;
+}
+// FP64 k_pcg_rows keeps S in registers and P^-1 in shared memory (SmemRows)
+template <typename T>
+__host__ __device__ constexpr bool pcg_p_in_smem()
+{
+    return sizeof(T) == 8;
+}
+// rows per thread of the cluster PCG (both matrices in registers)
+template <typename T>
+__host__ __device__ constexpr int cluster_rows_per_thread()
+{
     return sizeof(T) == 4 ? 2 : 1;
 }
 
-template <int NQ>
+
+template <int NQ, int RPT>
 struct SmemRows;
 
 template <int NQ, int RPT>
@@ -558,19 +578,14 @@ struct RowPcg {
     static constexpr int MAX_THREADS = 512 / RPT;
     __host__ __device__ static int threads(int N) { return ((N * TPB + 31) / 32) * 32; }
     __host__ __device__ static bool fits(int N) { return N * TPB <= MAX_THREADS; }
+    // the two CG vectors and the reduction slots; in FP64 also P^-1
+    // (SmemRows, pcg_p_in_smem)
     template <typename T>
     __host__ __device__ static size_t smem_bytes(int N)
     {
-        return 2 * (size_t)(N + 2) * VS * sizeof(T) + 2 * WARP * sizeof(double) + 16;
-    }
-    // FP64 with P^-1 in shared memory (k_pcg_rows_psm): one row per thread,
-    // at most PSM_THREADS threads (registers for S: 65536 / 448 = 146 a thread)
-    static constexpr int PSM_THREADS = 448;
-    __host__ __device__ static bool fits_psm(int N) { return RPT == 1 && N * TPB <= PSM_THREADS; }
-    __host__ __device__ static size_t smem_bytes_psm(int N)
-    {
-        return smem_bytes<double>(N) + 16 +
-               (size_t)RD * SmemRows<NQ>::stride(threads(N)) * sizeof(double);
+        const size_t base = 2 * (size_t)(N + 2) * VS * sizeof(T) + 2 * WARP * sizeof(double) + 16;
+        if (!pcg_p_in_smem<T>()) return base;
+        return base + 16 + (size_t)N * n * RD * sizeof(double);
     }
 };
 
@@ -669,53 +684,48 @@ __device__ __forceinline__ void rows_window_dot(const RowMat<NQ, RPT, float>& ro
                  ((acc[j][2].x + acc[j][2].y) + (acc[j][3].x + acc[j][3].y));
 }
 
-// FP64 P^-1 rows in shared memory, one row per thread.  An FP64 problem's S
-// and P^-1 (2 x 150 KB for iiwa14 N = 32) do not fit in one SM's registers
-// together: S stays in registers and P^-1 is stored transposed, entry (row r,
-// column c) of the [N n][3n] block-row layout at pt[c * rs + r], rs = the
-// CTA's thread count + 1 (odd).  A warp's load of one column then reads 32
-// consecutive doubles (two wavefronts, no conflicts), and the cooperative
-// fill, which walks the global rows in order, spreads its stores over the
-// banks.  The dot product keeps the register form's four partial sums by
-// column mod 4, so the iterates are those of k_pcg_rows bit for bit.
-template <int NQ>
+// FP64 P^-1 in shared memory.  An FP64 problem's S and P^-1 (2 x 150 KB for
+// iiwa14 N = 32) do not fit in one SM's registers together: S stays in
+// registers (RPT rows a thread) and P^-1 is bulk-copied into shared memory
+// in its global layout, row-major [N n][3n].  A row is 3n doubles = 21
+// sixteen-byte chunks for iiwa14 (an odd count), so the 16-byte loads of
+// eight threads on consecutive rows fall in eight different bank quads.  The
+// dot product keeps the register form's four partial sums by column mod 4
+// and reads each window value once for the thread's RPT rows, so the iterates
+// are those of the register form bit for bit.
+template <int NQ, int RPT>
 struct SmemRows {
-    static constexpr int n = 2 * NQ, RD = 3 * n;
-    double* pt;
-    int rs, row;
-    // every thread of the CTA: rows [0, nrows) of src into pt, zero rows up
-    // to the thread count; a barrier must follow before the first dot
-    __device__ __forceinline__ void fill(const double* __restrict__ src, int nrows) const
-    {
-        const int total = nrows * RD;
-        for (int e = threadIdx.x; e < total; e += blockDim.x) {
-            const int r = e / RD, c = e - r * RD;
-            pt[c * rs + r] = src[e];
-        }
-        for (int r = nrows + threadIdx.x; r < (int)blockDim.x; r += blockDim.x)
-#pragma unroll
-            for (int c = 0; c < RD; ++c) pt[c * rs + r] = 0.0;
-    }
-    __host__ __device__ static int stride(int threads) { return threads + 1; }
+    static constexpr int n = 2 * NQ, RD = 3 * n, TPB = n / RPT;
+    const double* base;  // the problem's P^-1 in shared memory
+    int row0;            // the thread's rows: row0 + j * TPB
 };
 
-template <int NQ>
-__device__ __forceinline__ void rows_window_dot(const SmemRows<NQ>& p, const double* win,
-                                                double (&out)[1])
+template <int NQ, int RPT>
+__device__ __forceinline__ void rows_window_dot(const SmemRows<NQ, RPT>& p, const double* win,
+                                                double (&out)[RPT])
 {
-    constexpr int n = 2 * NQ, VS = row_vs(n);
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    const double* col = p.pt + p.row;
+    constexpr int n = 2 * NQ, VS = row_vs(n), TPB = n / RPT, RD = 3 * n;
+    double acc[RPT][4];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j)
+#pragma unroll
+        for (int a = 0; a < 4; ++a) acc[j][a] = 0.0;
 #pragma unroll
     for (int blk = 0; blk < 3; ++blk) {
 #pragma unroll
         for (int c0 = 0; c0 < n; c0 += 2) {
             const double2 v = *reinterpret_cast<const double2*>(win + blk * VS + c0);
-            acc[c0 & 3] += col[(blk * n + c0) * p.rs] * v.x;
-            acc[(c0 + 1) & 3] += col[(blk * n + c0 + 1) * p.rs] * v.y;
+#pragma unroll
+            for (int j = 0; j < RPT; ++j) {
+                const double2 m = *reinterpret_cast<const double2*>(
+                    p.base + (size_t)(p.row0 + j * TPB) * RD + blk * n + c0);
+                acc[j][c0 & 3] += m.x * v.x;
+                acc[j][(c0 + 1) & 3] += m.y * v.y;
+            }
         }
     }
-    out[0] = (acc[0] + acc[1]) + (acc[2] + acc[3]);
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) out[j] = (acc[j][0] + acc[j][1]) + (acc[j][2] + acc[j][3]);
 }
 
 template <typename Acc>
@@ -768,8 +778,12 @@ struct NoDzStage {
 // A_k and Qi_k blocks in shared memory, used by the step recovery on the
 // threads where dz_ready() returns true (each thread decides for itself; no
 // barrier depends on it), else read from global memory.
+// PSM: P^-1 in shared memory (SmemRows, FP64), S in registers.  An FP64
+// problem's S and P^-1 (2 x 150 KB for iiwa14 N = 32) do not fit one SM's
+// registers together; the FP64 form with both in registers (one row a
+// thread) spilled and ran the PCG in 10.8 ms per solve, this one in 9.9.
 template <int NQ, typename T, typename Acc, int RPT, class Hook = NoHook,
-          class DzReady = NoDzStage, bool PSM = false>
+          class DzReady = NoDzStage, bool PSM = pcg_p_in_smem<T>()>
 __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int it_row,
                                               unsigned char* smem_raw, const T* Sp = nullptr,
                                               const T* Pp = nullptr, Hook hook = Hook(),
@@ -789,6 +803,22 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
     T* pv = reinterpret_cast<T*>(smem_raw);
     T* rv = pv + L;
     Acc* red = reinterpret_cast<Acc*>(((uintptr_t)(rv + L) + 15) & ~(uintptr_t)15);
+    // PSM: the bulk copies' mbarrier and the broadcast outcome of a wait
+    __shared__ __align__(8) uint64_t s_pbar;
+    __shared__ int s_pok;
+    auto stage_wait = [&](uint32_t parity) {  // every thread; false: the wait expired
+        if (tid == 0) {
+            s_pok = mbar_wait_bounded(&s_pbar, parity, bt.wait_tries);
+            if (!s_pok) {
+                atomicExch(bt.work + 2, 1);
+                if (mbar_wait_bounded(&s_pbar, parity, PCG_STAGE_DRAIN_TRIES)) mbar_inval(&s_pbar);
+            }
+        }
+        __syncthreads();
+        if (!s_pok) return false;
+        if (tid != 0) mbar_try_wait(&s_pbar, parity);  // phase complete: acquires the data
+        return true;
+    };
     for (int j = tid; j < 2 * L; j += blockDim.x) pv[j] = T(0);
     T* lam = bt.lambda + (size_t)b * d.vecp();
     const int w0 = k * VS;
@@ -797,22 +827,44 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
 #pragma unroll
     for (int j = 0; j < RPT; ++j) x[j] = act ? lam[(k + 1) * n + i0 + j * TPB] : T(0);
     if (!bt.conv[b]) {
-        // PSM: P^-1 in shared memory after the reduction slots (FP64, RPT = 1)
-        static_assert(!PSM || (RPT == 1 && sizeof(T) == 8), "P^-1 in shared memory is FP64");
+        // PSM: one shared-memory buffer after the reduction slots takes S by
+        // bulk copy, the threads load their S rows from it into registers,
+        // then it takes P^-1 (the second copy runs while r = gamma - S x is
+        // formed).  Thread 0 waits with a bound and broadcasts the outcome; an
+        // expired wait sets bt.work[2] (the host reports GATO_ERR_TIMEOUT and
+        // the launch's results are not valid), lets the copy land and ends the
+        // problem.
+        static_assert(!PSM || sizeof(T) == 8, "P^-1 in shared memory is FP64");
         RowMat<NQ, RPT, T> srow;
-        std::conditional_t<PSM, SmemRows<NQ>, RowMat<NQ, RPT, T>> prow;
+        std::conditional_t<PSM, SmemRows<NQ, RPT>, RowMat<NQ, RPT, T>> prow;
         {
             const size_t row = (size_t)(k * n + i0) * RD;
             const size_t prob = (size_t)b * d.b3d();
-            srow.load((Sp ? Sp : bt.S + prob) + row, (size_t)TPB * RD, act);
+            const T* Sg = Sp ? Sp : bt.S + prob;
+            const T* Pg = Pp ? Pp : bt.P + prob;
             if constexpr (PSM) {
-                prow.pt = reinterpret_cast<double*>(
-                    ((uintptr_t)(red + 2 * WARP) + 15) & ~(uintptr_t)15);
-                prow.rs = SmemRows<NQ>::stride(blockDim.x);
-                prow.row = tid;
-                prow.fill(reinterpret_cast<const double*>(Pp ? Pp : bt.P + prob), N * n);
+                T* buf = reinterpret_cast<T*>(((uintptr_t)(red + 2 * WARP) + 15) & ~(uintptr_t)15);
+                const uint32_t bytes = (uint32_t)(d.b3d() * sizeof(T));
+                if (tid == 0) {
+                    mbar_init(&s_pbar, 1);
+                    fence_mbar_init();
+                    fence_proxy_async_shared();
+                    mbar_arrive_expect_tx(&s_pbar, bytes);
+                    bulk_copy_g2s(buf, Sg, bytes, &s_pbar);
+                }
+                if (!stage_wait(0)) return;
+                srow.load(buf + row, (size_t)TPB * RD, act);
+                __syncthreads();  // every S read of the buffer is done
+                if (tid == 0) {
+                    fence_proxy_async_shared();
+                    mbar_arrive_expect_tx(&s_pbar, bytes);
+                    bulk_copy_g2s(buf, Pg, bytes, &s_pbar);
+                }
+                prow.base = buf;
+                prow.row0 = k * n + i0;
             } else {
-                prow.load((Pp ? Pp : bt.P + prob) + row, (size_t)TPB * RD, act);
+                srow.load(Sg + row, (size_t)TPB * RD, act);
+                prow.load(Pg + row, (size_t)TPB * RD, act);
             }
         }
         T g[RPT], r[RPT], z[RPT], p[RPT], ap[RPT];
@@ -832,7 +884,11 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
             r[j] = act ? g[j] - r[j] : T(0);
             if (act) rv[(k + 1) * VS + i0 + j * TPB] = r[j];
         }
-        __syncthreads();
+        if constexpr (PSM) {
+            if (!stage_wait(1)) return;  // P^-1 landed (the wait is also the barrier)
+        } else {
+            __syncthreads();
+        }
         rows_window_dot(prow, rv + w0, z);
         const Acc abs_tol = Acc(bt.abs_tol);
         const T eps = bt.tol[b];
@@ -966,6 +1022,9 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
     // res_x = q_k - lambda_k + A_k^T lambda_{k+1}, dz_x = -Qi_k res_x,
     // res_u = r_k + B_k^T lambda_{k+1}, dz_u = -Ri_k res_u
     __syncthreads();
+    if constexpr (PSM) {
+        if (tid == 0 && !bt.conv[b]) mbar_inval(&s_pbar);  // both copies landed
+    }
     if constexpr (HOOK) hook();
     if (act) {
 #pragma unroll
@@ -1048,18 +1107,6 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
     pcg_rows_body<NQ, T, Acc, RPT>(bt, blockIdx.x, it_row, smem_raw);
 }
 
-// FP64 k_pcg_rows with S in registers and P^-1 in shared memory (one row per
-// thread; the register form of FP64 holds both and spills).  Same iterates.
-// (at most PSM_THREADS = 448 threads: 14 warps, four on one of the SM's four
-// 16K-register partitions, so 128 registers a thread)
-template <int NQ, typename Acc>
-__global__ void __launch_bounds__(RowPcg<NQ, 1>::PSM_THREADS, 1)
-    k_pcg_rows_psm(Batch<NQ, double> bt, int it_row)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    pcg_rows_body<NQ, double, Acc, 1, NoHook, NoDzStage, true>(bt, blockIdx.x, it_row, smem_raw);
-}
-
 // Persistent FP32 form of k_pcg_rows: one CTA per SM takes problems from a
 // counter (bt.work[0]).  When a problem's CG loop ends, the CTA claims the
 // next problem and the bulk-copy engine brings its S and P^-1 (2 x 12 N NQ^2
@@ -1101,8 +1148,6 @@ struct PcgStage {
     }
 };
 
-constexpr int PCG_STAGE_WAIT_TRIES = 1 << 22;   // default bound: seconds
-constexpr int PCG_STAGE_DRAIN_TRIES = 1 << 22;
 
 template <int NQ, typename Acc>
 __global__ void __launch_bounds__(RowPcg<NQ, 2>::MAX_THREADS, 1)
@@ -1412,8 +1457,11 @@ __device__ __forceinline__ void fused_iter_body(const Batch<NQ, T>& bt, const De
     }
 }
 
+// Resident CTAs per SM: four in FP32 (64 registers), two in FP64 (128
+// registers; both spill, and both are faster than fewer CTAs without spills:
+// FP64 5.36 against 6.48 ms per solve with one CTA at 255 registers)
 template <int NQ, typename T, typename Acc>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
     k_fused_iter(Batch<NQ, T> bt, DevModel<NQ, T> M, int stage, int it_row, int with_pcg,
                  int with_kkt)
 {

@@ -508,18 +508,6 @@ bool pcg_stream_dz_fits(const gato_solver* s)
         return false;
 }
 
-// FP64 runs k_pcg_rows_psm (S in registers, P^-1 in shared memory) where
-// one row per thread fits its thread limit and P^-1 fits shared memory
-template <class Tg>
-bool pcg_psm_fits(const gato_solver* s)
-{
-    if constexpr (sizeof(typename Tg::T) == 8)
-        return RowPcg<Tg::NQ, 1>::fits_psm(s->N) &&
-               RowPcg<Tg::NQ, 1>::smem_bytes_psm(s->N) <= (size_t)s->max_smem;
-    else
-        return false;
-}
-
 // register-resident PCG + dz of every problem
 template <class Tg>
 void launch_pcg_rows(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt,
@@ -539,13 +527,6 @@ void launch_pcg_rows(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typena
             return;
         }
     }
-    if constexpr (sizeof(T) == 8) {
-        if (pcg_psm_fits<Tg>(s)) {
-            k_pcg_rows_psm<NQ, Acc><<<s->B, RowPcg<NQ, 1>::threads(s->N),
-                                      RowPcg<NQ, 1>::smem_bytes_psm(s->N), st>>>(bt, row);
-            return;
-        }
-    }
     constexpr int RPT = pcg_rows_per_thread<T>();
     k_pcg_rows<NQ, T, Acc, RPT><<<s->B, RowPcg<NQ, RPT>::threads(s->N),
                                    RowPcg<NQ, RPT>::template smem_bytes<T>(s->N), st>>>(bt, row);
@@ -559,7 +540,7 @@ int launch_pcg_cluster(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, type
     constexpr int NQ = Tg::NQ;
     using T = typename Tg::T;
     using Acc = typename Tg::Acc;
-    constexpr int RPT = pcg_rows_per_thread<T>();
+    constexpr int RPT = cluster_rows_per_thread<T>();
     using CP = ClusterPcg<NQ, RPT>;
     ProfScope ps_(s, st, GATO_KERNEL_PCG);
     const int C = CP::ctas(s->N);
@@ -586,8 +567,8 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
     constexpr int NQ = Tg::NQ;
     using T = typename Tg::T;
     using Acc = typename Tg::Acc;
-    // rows of S and P^-1 per thread in k_pcg_rows: two in FP32 (each window
-    // value loaded from shared memory feeds two rows), one in FP64 (registers)
+    // rows of S and P^-1 per thread in k_pcg_rows: two (each window value
+    // loaded from shared memory feeds two rows)
     constexpr int RPT = pcg_rows_per_thread<T>();
     // Up to 1.5 problems per SM, one CTA per problem would leave SMs idle
     // and make every problem's KKT blocks and Schur complement serial chains
@@ -613,7 +594,7 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
         CKL();
         return GATO_OK;
     }
-    if (ClusterPcg<NQ, RPT>::fits(s->N)) {
+    if (ClusterPcg<NQ, cluster_rows_per_thread<T>()>::fits(s->N)) {
         if (with_kkt) {
             ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
             FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, false};
@@ -672,13 +653,9 @@ int configure_kernels(gato_solver* s)
                     lay.bytes());
     RC(set_smem(k_fused_iter<NQ, T, Acc>, lay.bytes(), s->max_smem));
     constexpr int RPT = pcg_rows_per_thread<T>();
-    RC(set_smem(k_pcg_rows<NQ, T, Acc, RPT>, RowPcg<NQ, RPT>::template smem_bytes<T>(s->N),
-                s->max_smem));
-    if constexpr (sizeof(T) == 8) {
-        if (pcg_psm_fits<Tg>(s))
-            RC(set_smem(k_pcg_rows_psm<NQ, Acc>, RowPcg<NQ, 1>::smem_bytes_psm(s->N),
-                        s->max_smem));
-    }
+    if (RowPcg<NQ, RPT>::fits(s->N))  // longer horizons take the cluster PCG
+        RC(set_smem(k_pcg_rows<NQ, T, Acc, RPT>, RowPcg<NQ, RPT>::template smem_bytes<T>(s->N),
+                    s->max_smem));
     if constexpr (sizeof(T) == 4) {
         if (pcg_stream_fits<Tg>(s))
             RC(set_smem(k_pcg_rows_stream<NQ, Acc>,
@@ -918,7 +895,8 @@ int pcg_and_step(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename T
         CKL();
         return GATO_OK;
     }
-    if (ClusterPcg<NQ, RPT>::fits(s->N)) return launch_pcg_cluster<Tg>(s, st, bt, -1);
+    if (ClusterPcg<NQ, cluster_rows_per_thread<T>()>::fits(s->N))
+        return launch_pcg_cluster<Tg>(s, st, bt, -1);
     RC(launch_pcg<Tg>(s, st, bt, -1));
     return launch_dz<Tg>(s, st, bt);
 }
