@@ -559,6 +559,10 @@ __host__ __device__ constexpr bool pcg_p_in_smem()
 {
     return sizeof(T) == 8;
 }
+// experiment: lanes per knot of the FP64 KKT stage in k_fused_iter
+#ifndef GATO_FP64_KG
+#define GATO_FP64_KG 16
+#endif
 // rows per thread of the cluster PCG (both matrices in registers)
 template <typename T>
 __host__ __device__ constexpr int cluster_rows_per_thread()
@@ -693,6 +697,14 @@ __device__ __forceinline__ void rows_window_dot(const RowMat<NQ, RPT, float>& ro
 // dot product keeps the register form's four partial sums by column mod 4
 // and reads each window value once for the thread's RPT rows, so the iterates
 // are those of the register form bit for bit.
+// horizons whose PCG runs k_pcg_rows (one CTA a problem); longer ones take
+// the cluster PCG
+template <int NQ, typename T>
+__host__ __device__ bool rows_pcg_fits(int N)
+{
+    return RowPcg<NQ, pcg_rows_per_thread<T>()>::fits(N);
+}
+
 template <int NQ, int RPT>
 struct SmemRows {
     static constexpr int n = 2 * NQ, RD = 3 * n, TPB = n / RPT;
@@ -1466,7 +1478,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
                  int with_kkt)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    fused_iter_body<NQ, T, Acc>(bt, M, blockIdx.x, stage, it_row, with_pcg, smem_raw,
+    fused_iter_body<NQ, T, Acc, (sizeof(T) == 8 ? GATO_FP64_KG : 16)>(bt, M, blockIdx.x, stage, it_row, with_pcg, smem_raw,
                                 Team::cta(), with_kkt != 0);
 }
 

@@ -43,8 +43,7 @@ void mixed_args(gato_mixed* mx, void* const* xu, const void* const* xs, const vo
 template <typename T>
 bool rows_fit(const gato_solver* s)
 {
-    constexpr int RPT = pcg_rows_per_thread<T>();
-    return s->nq == 7 ? RowPcg<7, RPT>::fits(s->N) : RowPcg<6, RPT>::fits(s->N);
+    return s->nq == 7 ? rows_pcg_fits<7, T>(s->N) : rows_pcg_fits<6, T>(s->N);
 }
 
 template <typename T, typename Acc, int KG, int PPB, int MINB>

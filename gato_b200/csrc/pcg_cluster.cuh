@@ -1,8 +1,8 @@
 // Register-resident PCG for long horizons: one thread-block cluster per
 // problem.  The S and P^-1 rows of N knots do not fit one SM's registers
 // beyond N ~ 36 (iiwa14), so the block rows are split across a cluster of
-// C = ceil(N / 32) CTAs (C <= 8), each holding up to 32 block rows exactly as
-// k_pcg_rows does.  CG vectors live in each CTA's shared memory with one halo
+// C = ceil(N / 32) CTAs (C <= 8; FP64 ceil(N / 16)), each holding up to 32
+// (16) block rows exactly as k_pcg_rows does.  CG vectors live in each CTA's shared memory with one halo
 // block on each side; the owner of a boundary block also stores it into the
 // neighbour CTA's halo through distributed shared memory, and a cluster
 // barrier publishes it.  Reductions sum per CTA, every CTA writes its partial
@@ -22,7 +22,11 @@ template <int NQ, int RPT>
 struct ClusterPcg {
     static constexpr int n = 2 * NQ, m = NQ, RD = 3 * n, VS = row_vs(n);
     static constexpr int TPB = n / RPT;
-    static constexpr int MAX_ROWS = 32;    // block rows per CTA
+    // block rows per CTA: 32 with two rows a thread (FP32); 16 with one (FP64),
+    // so that a thread's S and P^-1 rows (2 x 42 doubles for iiwa14) stay
+    // within 255 registers at 224 threads
+    static constexpr int MAX_ROWS = RPT == 1 ? 16 : 32;
+    static constexpr int MAX_THREADS = 256;
     static constexpr int MAX_CLUSTER = 8;  // portable cluster size
     __host__ __device__ static int ctas(int N) { return (N + MAX_ROWS - 1) / MAX_ROWS; }
     __host__ __device__ static int rows(int N)
@@ -45,7 +49,7 @@ struct ClusterPcg {
 };
 
 template <int NQ, typename T, typename Acc, int RPT>
-__global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
+__global__ void __launch_bounds__(ClusterPcg<NQ, RPT>::MAX_THREADS, 1)
     k_pcg_cluster(Batch<NQ, T> bt, int it_row)
 {
     namespace cg = cooperative_groups;

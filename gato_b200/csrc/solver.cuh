@@ -578,7 +578,7 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
     // 90.7K; B = 192 110.2K -> 113.2K; B = 256 125.6K -> 116.8K.
     const int with_kkt = 2 * s->B > 3 * s->nsm;
     if (!with_kkt) RC(launch_kkt<Tg>(s, st, bt));
-    if (RowPcg<NQ, RPT>::fits(s->N)) {
+    if (rows_pcg_fits<NQ, T>(s->N)) {
         // KKT + Schur into global memory, then the register-resident PCG + dz
         if (with_kkt) {
             ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
@@ -653,7 +653,7 @@ int configure_kernels(gato_solver* s)
                     lay.bytes());
     RC(set_smem(k_fused_iter<NQ, T, Acc>, lay.bytes(), s->max_smem));
     constexpr int RPT = pcg_rows_per_thread<T>();
-    if (RowPcg<NQ, RPT>::fits(s->N))  // longer horizons take the cluster PCG
+    if (rows_pcg_fits<NQ, T>(s->N))  // longer horizons take the cluster PCG
         RC(set_smem(k_pcg_rows<NQ, T, Acc, RPT>, RowPcg<NQ, RPT>::template smem_bytes<T>(s->N),
                     s->max_smem));
     if constexpr (sizeof(T) == 4) {
@@ -889,7 +889,7 @@ int pcg_and_step(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename T
     using T = typename Tg::T;
     using Acc = typename Tg::Acc;
     constexpr int RPT = pcg_rows_per_thread<T>();
-    if (RowPcg<NQ, RPT>::fits(s->N)) {
+    if (rows_pcg_fits<NQ, T>(s->N)) {
         ProfScope ps_(s, st, GATO_KERNEL_PCG);
         launch_pcg_rows<Tg>(s, st, bt, -1);
         CKL();

@@ -254,11 +254,12 @@ int gato_set_pcg_tol_batch(gato_solver_t* s, const float* h_tol);
    as PyBSQP::solve does). */
 int gato_set_dt(gato_solver_t* s, float dt);
 
-/* Bounds of the device-side waits of the persistent FP32 PCG (no
-   counterpart in the reference, which has no bulk copies): how many
+/* Bounds of the device-side waits of the PCG kernels that bring S and P^-1
+   into shared memory by bulk copy, the persistent FP32 PCG and the FP64 PCG
+   (no counterpart in the reference, which has no bulk copies): how many
    mbarrier try_wait calls (each suspends the waiting thread for at most about
    a microsecond) a CTA makes before it gives up on a problem's S / P^-1
-   copy (copy_tries) and on the step recovery's A_k / Qi_k copy
+   copy (copy_tries) and, FP32 only, on the step recovery's A_k / Qi_k copy
    (step_copy_tries).  A wait that gives up lets the copies in flight land,
    and the next synchronising call on the handle returns GATO_ERR_TIMEOUT
    (the results of that solve are not valid).  A negative value restores

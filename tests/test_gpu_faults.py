@@ -135,3 +135,31 @@ def test_expired_copy_wait_reports_timeout(limits):
     s.close()
     np.testing.assert_array_equal(again["XU"], clean["XU"])
     np.testing.assert_array_equal(again["pcg_iters"], clean["pcg_iters"])
+
+
+def test_expired_copy_wait_reports_timeout_fp64():
+    """The FP64 PCG (S and P^-1 brought into shared memory by bulk copy) told
+    to give up at once on its copy wait: the solve reports GATO_ERR_TIMEOUT,
+    the kernel lets the copy land before the CTA ends, and after the default
+    bound is restored the same handle solves exactly as before."""
+    import gato_b200
+    plant, N, B = "iiwa14", 32, 300
+    pr = problem(plant, N, B, seed=67)
+    s = gpu_solver(plant, N, B, form="fused", precision="fp64", **PARAMS_CFG2)
+    lam0 = s.get_lambda()
+
+    def run():
+        s.set_lambda(lam0)
+        s.reset_rho()
+        return s.solve_raw(pr["xu"].astype(np.float64), 0.01, pr["xs"].astype(np.float64),
+                           pr["goal"].astype(np.float64))
+
+    clean = run()
+    s.set_wait_limits(0, -1)
+    with pytest.raises(gato_b200.GatoError, match="error -5"):
+        run()
+    s.set_wait_limits(-1, -1)
+    again = run()
+    s.close()
+    np.testing.assert_array_equal(again["XU"], clean["XU"])
+    np.testing.assert_array_equal(again["pcg_iters"], clean["pcg_iters"])
