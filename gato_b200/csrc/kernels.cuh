@@ -559,10 +559,6 @@ __host__ __device__ constexpr bool pcg_p_in_smem()
 {
     return sizeof(T) == 8;
 }
-// experiment: lanes per knot of the FP64 KKT stage in k_fused_iter
-#ifndef GATO_FP64_KG
-#define GATO_FP64_KG 16
-#endif
 // rows per thread of the cluster PCG (both matrices in registers)
 template <typename T>
 __host__ __device__ constexpr int cluster_rows_per_thread()
@@ -1369,7 +1365,11 @@ struct Team {
 // KG: lanes per knot in the KKT stage (16: two knots per warp, 32: one).
 // `team` is the set of warps working on this problem (the whole CTA, or half
 // of it when a CTA runs two problems at once); with_pcg needs the whole CTA.
-template <int NQ, typename T, typename Acc, int KG = 16>
+// KKT_STAGE / SCHUR_STAGE compile the KKT set-up and the Schur stage (with
+// the PCG when with_pcg) in or out, so a kernel that runs one of them is
+// allocated the registers of that one alone.
+template <int NQ, typename T, typename Acc, int KG = 16, bool KKT_STAGE = true,
+          bool SCHUR_STAGE = true>
 __device__ __forceinline__ void fused_iter_body(const Batch<NQ, T>& bt, const DevModel<NQ, T>& M,
                                                 int b, int stage, int it_row, int with_pcg,
                                                 unsigned char* smem_raw,
@@ -1409,7 +1409,7 @@ __device__ __forceinline__ void fused_iter_body(const Batch<NQ, T>& bt, const De
 
     // KKT set-up, two knots per warp (one per half-warp) or one per warp;
     // skipped when a knot-parallel KKT kernel already wrote the blocks
-    if (!with_kkt) {
+    if (!KKT_STAGE || !with_kkt) {
     } else if constexpr (KG == 32) {
         for (int k = wid; k < N - 1; k += nw)
             kkt_knot<NQ, T, 32>(M, cost_of<NQ>(bt.cp, b), N, k, xu, bt.xs + (size_t)b * nx,
@@ -1426,6 +1426,7 @@ __device__ __forceinline__ void fused_iter_body(const Batch<NQ, T>& bt, const De
                                 ws + half * KktSmem<NQ>::SIZE, valid);
         }
     }
+    if constexpr (!SCHUR_STAGE) return;
     team.sync();
     for (int k = wid; k < N; k += nw) {
         warp_invert<nx, T>(Q + k * nx * nx, rho, Qi + k * nx * nx);
@@ -1478,8 +1479,33 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
                  int with_kkt)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    fused_iter_body<NQ, T, Acc, (sizeof(T) == 8 ? GATO_FP64_KG : 16)>(bt, M, blockIdx.x, stage, it_row, with_pcg, smem_raw,
+    fused_iter_body<NQ, T, Acc>(bt, M, blockIdx.x, stage, it_row, with_pcg, smem_raw,
                                 Team::cta(), with_kkt != 0);
+}
+
+// The two halves of k_fused_iter as separate kernels (CTA per problem, same
+// shared-memory layout): the KKT set-up, whose dynamics derivatives need the
+// registers (FP32: two CTAs per SM, 128 registers, 720 B spilled; FP64: one,
+// 255), and the Schur stage (FP32: four CTAs per SM at 64 registers without
+// spills; FP64: two).  The KKT blocks pass through L2 between them.  Against
+// the one kernel that does both (FP32 at 64 registers, 2 KB spilled; FP64 at
+// 128, 3.8 KB), iiwa14 N = 32 B = 1024, per solve: FP32 2.33 -> 2.03 ms,
+// FP64 5.42 -> 3.81 ms; the KKT half at three CTAs per SM (80 registers):
+// FP32 2.18 ms.
+template <int NQ, typename T, typename Acc>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+    k_fused_kkt(Batch<NQ, T> bt, DevModel<NQ, T> M, int it_row)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    fused_iter_body<NQ, T, Acc, 16, true, false>(bt, M, blockIdx.x, 0, it_row, 0, smem_raw);
+}
+template <int NQ, typename T, typename Acc>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
+    k_fused_schur(Batch<NQ, T> bt, DevModel<NQ, T> M, int it_row)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    fused_iter_body<NQ, T, Acc, 16, false, true>(bt, M, blockIdx.x, 0, it_row, 0, smem_raw,
+                                                  Team::cta(), false);
 }
 
 }  // namespace gato

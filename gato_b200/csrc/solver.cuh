@@ -560,6 +560,24 @@ int launch_pcg_cluster(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, type
     return GATO_OK;
 }
 
+// KKT blocks and Schur system of every problem, CTA per problem, S and P^-1
+// to global memory, as the two halves of k_fused_iter (k_fused_kkt, then
+// k_fused_schur), each compiled for its own occupancy
+template <class Tg>
+int launch_kkt_schur(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt,
+                     int row)
+{
+    constexpr int NQ = Tg::NQ;
+    using T = typename Tg::T;
+    using Acc = typename Tg::Acc;
+    ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
+    FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, false};
+    k_fused_kkt<NQ, T, Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(bt, dmodel<Tg>(s), row);
+    k_fused_schur<NQ, T, Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(bt, dmodel<Tg>(s), row);
+    CKL();
+    return GATO_OK;
+}
+
 template <class Tg>
 int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typename Tg::T>& bt,
                       int row)
@@ -581,11 +599,7 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
     if (rows_pcg_fits<NQ, T>(s->N)) {
         // KKT + Schur into global memory, then the register-resident PCG + dz
         if (with_kkt) {
-            ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
-            FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, false};
-            k_fused_iter<NQ, T, Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(
-                bt, dmodel<Tg>(s), 0, row, 0, 1);
-            CKL();
+            RC(launch_kkt_schur<Tg>(s, st, bt, row));
         } else {
             RC(launch_schur<Tg>(s, st, bt));
         }
@@ -596,11 +610,7 @@ int launch_fused_iter(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typen
     }
     if (ClusterPcg<NQ, cluster_rows_per_thread<T>()>::fits(s->N)) {
         if (with_kkt) {
-            ProfScope ps_(s, st, GATO_KERNEL_FUSED_ITER);
-            FusedLayout<NQ, T> lay{s->N, FUSED_THREADS / WARP, false};
-            k_fused_iter<NQ, T, Acc><<<s->B, FUSED_THREADS, lay.bytes(), st>>>(
-                bt, dmodel<Tg>(s), 0, row, 0, 1);
-            CKL();
+            RC(launch_kkt_schur<Tg>(s, st, bt, row));
         } else {
             RC(launch_schur<Tg>(s, st, bt));
         }
@@ -652,6 +662,8 @@ int configure_kernels(gato_solver* s)
         return fail(GATO_ERR_UNSUPPORTED, "N=%d needs %zu bytes of shared memory", s->N,
                     lay.bytes());
     RC(set_smem(k_fused_iter<NQ, T, Acc>, lay.bytes(), s->max_smem));
+    RC(set_smem(k_fused_kkt<NQ, T, Acc>, lay.bytes(), s->max_smem));
+    RC(set_smem(k_fused_schur<NQ, T, Acc>, lay.bytes(), s->max_smem));
     constexpr int RPT = pcg_rows_per_thread<T>();
     if (rows_pcg_fits<NQ, T>(s->N))  // longer horizons take the cluster PCG
         RC(set_smem(k_pcg_rows<NQ, T, Acc, RPT>, RowPcg<NQ, RPT>::template smem_bytes<T>(s->N),
