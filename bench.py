@@ -44,9 +44,10 @@ sys.path.insert(0, ROOT)
 
 PLANT, N, DT = "iiwa14", 32, 0.01
 # DRAM bytes (read + write) per launch from one ncu capture of the first SQP
-# iteration of this workload (profiles/k_fused_iter_iiwa14_N32_B1024.md,
-# profiles/k_pcg_rows_stream_iiwa14_N32_B1024.md)
-TRAFFIC_PER_LAUNCH = {"fused_iter": None, "pcg": 238_636_544}
+# iteration of this workload (profiles/k_fused_kkt_schur_iiwa14_N32_B1024.md,
+# profiles/k_pcg_rows_stream_iiwa14_N32_B1024.md); the KKT + Schur group is
+# both of its kernels
+TRAFFIC_PER_LAUNCH = {"fused_iter": 391_866_000, "pcg": 238_080_000}
 KERNEL_NAMES = {"fused_iter": "k_fused_kkt + k_fused_schur", "pcg": "k_pcg_rows_stream",
                 "line_search": "k_merit_ls", "merit": "k_merit_ls (one step size)"}
 # kernels per timed group of gato_profile_solve (the KKT + Schur group is two)
