@@ -1278,6 +1278,12 @@ def run_mpc(args):
                 r["grad_w_err_vs_fp64"] = float(np.abs(gw[ok] - ref["g_w"][ok]).max()
                                                 / np.abs(ref["g_w"][ok]).max())
                 r["grad_nonfinite_problems_on_fp64_traj"] = int((~ok).sum())
+                # the FP64 gradient's size where this precision's is not finite,
+                # beside its median size over all problems
+                gmax = np.abs(ref["g_w"]).max(axis=1)
+                r["fp64_grad_absmax_median"] = float(np.median(gmax))
+                r["fp64_grad_absmax_where_nonfinite"] = (
+                    [float(v) for v in gmax[~ok]] if (~ok).any() else [])
             res[prec] = r
             s.close()
         x64 = res["fp64"]["x"]
