@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(ClusterPcg<NQ, RPT>::MAX_THREADS, 1)
             csum2(rho, delta);
             if (!(fabs((double)rho) < (double)abs_tol)) {
                 const Acc rho_init = rho < 0 ? -rho : rho;
-                Acc alpha = rho / delta;
+                Acc alpha = rec_div(rho, delta);
                 const bool start = !(delta == 0);  // delta = 0: nothing to do
 #pragma unroll
                 for (int j = 0; j < RPT; ++j) {
@@ -192,9 +192,9 @@ __global__ void __launch_bounds__(ClusterPcg<NQ, RPT>::MAX_THREADS, 1)
                     csum2(rho_new, delta);
                     const Acc arn = rho_new < 0 ? -rho_new : rho_new;
                     if (arn < abs_tol + (Acc)eps * rho_init || !(arn > 0)) break;
-                    const Acc beta = rho_new / rho;
-                    const Acc rn_a = rho_new / alpha;  // independent of beta's division
-                    alpha = rho_new / (delta - beta * rn_a);
+                    const Acc beta = rec_div(rho_new, rho);
+                    const Acc rn_a = rec_div(rho_new, alpha);  // independent of beta's division
+                    alpha = rec_div(rho_new, delta - beta * rn_a);
                     // breakdown: keep the iterate (tested in Acc, no conversion on the
                     // loop's critical path)
                     if (!isfinite(alpha)) break;
