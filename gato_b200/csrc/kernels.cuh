@@ -1506,7 +1506,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
 // the one kernel that does both (FP32 at 64 registers, 2 KB spilled; FP64 at
 // 128, 3.8 KB), iiwa14 N = 32 B = 1024, per solve: FP32 2.33 -> 2.03 ms,
 // FP64 5.42 -> 3.81 ms; the KKT half at three CTAs per SM (80 registers):
-// FP32 2.18 ms.
+// FP32 2.18 ms; the FP64 KKT half at two CTAs (128 registers, 3.9 KB
+// spilled): 4.66 against 3.82 ms.
 template <int NQ, typename T, typename Acc>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     k_fused_kkt(Batch<NQ, T> bt, DevModel<NQ, T> M, int it_row)
