@@ -265,3 +265,44 @@ def test_fused_solve_repeats_exactly(plant, precision, B):
     assert (a["pcg_iters"][0] > 0).all()
     np.testing.assert_array_equal(a["XU"], b["XU"])
     np.testing.assert_array_equal(a["pcg_iters"], b["pcg_iters"])
+
+
+def test_fp32_counts_and_error_on_the_bench_workload(oracle_mod):
+    """The bench workload (iiwa14 N=32, perturbed converged warm start, five
+    SQP iterations), 256 problems, FP32 fused form against the FP64 oracle
+    from the same XU, lambda and rho: at least 95 % of the (problem,
+    iteration) PCG counts equal (96.2 % measured on all 1024 problems) and a
+    median trajectory error below 5e-4 (3.4e-4 measured), beside the oracle's
+    own FP32-storage floor on the same problems (every stored stage output
+    rounded to FP32, arithmetic FP64: 7.8e-5 measured), which this solver
+    may exceed by at most a factor of 8."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    import gato_b200
+    O = oracle_mod
+    B = 256
+    wl = bench.make_workload(B, seed=bench.replica_seed(0))
+    kw = bench.solver_kwargs()
+    s = gato_b200.BSQP(batch_size=B, N=bench.N, dt=bench.DT, plant_type=bench.PLANT,
+                       form="fused", precision="fp32", **kw)
+    s.set_lambda(wl["lam"])
+    s.reset_rho()
+    g = s.solve_raw(wl["xu"], bench.DT, wl["xs"], wl["goal"])
+    s.close()
+    runs = []
+    for flags in (0, 15):
+        ref = O.Solver(bench.PLANT, bench.N, B, O.make_params(dt=bench.DT, **kw), threads=8)
+        if flags:
+            ref.set_round_f32(flags)
+        ref.set_lambda(wl["lam"].astype(np.float64))
+        runs.append(ref.solve(wl["xu"].astype(np.float64), bench.DT,
+                              wl["xs"].astype(np.float64), wl["goal"].astype(np.float64)))
+    (xo, so), (xf, _) = runs
+    c = bench.compare_with_oracle(np.asarray(g["XU"], np.float64), g["pcg_iters"],
+                                  g["ls_step_size"], xo, so["pcg_iters"], so["ls_step_size"])
+    floor = float(np.median(bench.trajectory_errors(xf, xo)))
+    assert c["pcg_iters_equal_frac"] >= 0.95, c
+    assert c["xu_rel_err_median"] < 5e-4, c
+    assert c["xu_rel_err_median"] < 8 * floor, (c, floor)
