@@ -14,7 +14,8 @@ and L2 is flushed between steps.
             goals and D2H of XU inside the timed region)
   plain     solves/s of the plain per-kernel form, same workload
   by_precision  fused and plain solves/s in FP32, mixed (FP64 reductions)
-            and FP64
+            and FP64, the fused form's solves/s through the host API
+            (e2e_value), and each form's device time per kernel group
   roofline  FP32 CUDA-core roofline of the kernel with the largest share of
             device time (the persistent PCG, k_pcg_rows_stream)
   cpu_baseline  the FP64 oracle of the same SQP on the host cores, bounded
@@ -541,8 +542,36 @@ def precision_times(torch, dev, B, prec, wl, args, flush, stream):
         out.append(float(np.mean(time_device_steps(torch, s, bufs, wl, steps, max(1, args.warmup),
                                                    flush, stream))))
         kern[form] = profile_kernels(s, wl, bufs, stream)
+        if form == "fused":
+            kern["e2e_s"] = host_api_times(torch, s, wl, steps, max(1, args.warmup), flush)
         s.close()
     return out[0], out[1], kern
+
+
+def host_api_times(torch, solver, wl, steps, warmup, flush):
+    """Seconds per solve through the host API (gato_solve_host, or its _f64
+    form), pinned host buffers, H2D of XU, x0, goals and D2H of XU inside
+    the timed region; warm start restored and L2 flushed between solves."""
+    import gato_b200._lib as L
+    f64 = solver.precision == "fp64"
+    dt = torch.float64 if f64 else torch.float32
+    h_xu = torch.empty(tuple(wl["xu"].shape), dtype=dt).pin_memory()
+    h_xs = torch.tensor(wl["xs"], dtype=dt).pin_memory()
+    h_goal = torch.tensor(wl["goal"], dtype=dt).pin_memory()
+    fn = L.load().gato_solve_host_f64 if f64 else L.load().gato_solve_host
+    ptr = L.dptr if f64 else L.fptr
+    out = []
+    for i in range(warmup + steps):
+        h_xu.copy_(torch.from_numpy(wl["xu"]))
+        solver.set_lambda(wl["lam"])
+        solver.reset_rho()
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L.check(fn(solver._h, ptr(h_xu), DT, ptr(h_xs), ptr(h_goal), None))
+        if i >= warmup:
+            out.append(time.perf_counter() - t0)
+    return float(np.mean(out))
 
 
 def trajectory_errors(xg, xo):
@@ -918,7 +947,8 @@ def run_ours(args):
     # the other precisions' throughput on the same workload (fused and plain)
     by_prec = {args.precision: {"value": B / (float(np.mean(t_fused)) * 1e-3),
                                 "plain_value": B / (float(np.mean(t_plain)) * 1e-3),
-                                "fused_vs_plain": float(np.mean(t_plain) / np.mean(t_fused))}}
+                                "fused_vs_plain": float(np.mean(t_plain) / np.mean(t_fused)),
+                                "e2e_value": B / float(np.mean(e2e_times))}}
     kern_by_prec = {args.precision: {k: round(v["ms"], 4) for k, v in kern.items()
                                      if v["launches"]}}
     plain_kern_by_prec = {args.precision: None}
@@ -927,7 +957,7 @@ def run_ours(args):
             continue
         tf, tp, kp = precision_times(torch, dev, B, prec, wl, args, flush, stream)
         by_prec[prec] = {"value": B / (tf * 1e-3), "plain_value": B / (tp * 1e-3),
-                         "fused_vs_plain": tp / tf}
+                         "fused_vs_plain": tp / tf, "e2e_value": B / kp.pop("e2e_s")}
         kern_by_prec[prec] = {k: round(v["ms"], 4) for k, v in kp["fused"].items()
                               if v["launches"]}
         plain_kern_by_prec[prec] = {k: round(v["ms"], 4) for k, v in kp["plain"].items()
@@ -1028,6 +1058,7 @@ def run_ours(args):
             best = max(ok, key=lambda p: by_prec[p]["value"])
             line["at_1e-4"] = {"precision": best, "form": "fused (CUDA graph)",
                                "value": by_prec[best]["value"], "unit": "solves/s",
+                               "e2e_value": by_prec[best]["e2e_value"],
                                "plain_value": by_prec[best]["plain_value"],
                                "fused_vs_plain": by_prec[best]["fused_vs_plain"],
                                "xu_rel_err_median": accuracy[best]["xu_rel_err_median"],
