@@ -804,7 +804,8 @@ struct NoDzStage {
 // PSM: P^-1 in shared memory (SmemRows, FP64), S in registers.  An FP64
 // problem's S and P^-1 (2 x 150 KB for iiwa14 N = 32) do not fit one SM's
 // registers together; the FP64 form with both in registers (one row a
-// thread) spilled and ran the PCG in 10.8 ms per solve, this one in 9.9.
+// thread) spilled and ran the PCG in 10.8 ms per solve (iiwa14 N = 32,
+// 1024 problems), this one in 8.3.
 template <int NQ, typename T, typename Acc, int RPT, class Hook = NoHook,
           class DzReady = NoDzStage, bool PSM = pcg_p_in_smem<T>()>
 __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int it_row,
