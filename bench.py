@@ -23,8 +23,8 @@ and L2 is flushed between steps.
   accuracy_vs_fp64_oracle  every precision's trajectory error against the
             oracle, the oracle's own FP32-storage floor, and a converged
             (30-iteration) solve
-  at_1e-4   the fastest precision whose trajectories meet 1e-4 against the
-            oracle (median and 90th percentile), with its fused/plain ratio
+  at_1e-4   the fastest precision whose trajectories all meet 1e-4 against
+            the oracle (the largest error), with its fused/plain ratio
 
 `--impl reference` times the reference's algorithm on the host CPU (the FP64
 oracle port: the reference's solver has no CPU implementation and its CUDA
@@ -502,7 +502,19 @@ def time_device_steps(torch, solver, bufs, wl, steps, warmup, flush, stream):
     return np.array(times)
 
 
-PRECISIONS = ("fp32", "mixed", "fp64")
+PRECISIONS = ("fp32", "mixed", "fp64", "fp64-p32")
+
+
+def new_solver(prec, B, **kw):
+    """A fused- or plain-form solver of the workload's plant and horizon in
+    precision `prec`: "fp32", "mixed", "fp64", or "fp64-p32" (FP64 with the
+    preconditioner applied in FP32, gato_set_fp32_preconditioner)."""
+    import gato_b200
+    s = gato_b200.BSQP(batch_size=B, N=N, dt=DT, plant_type=PLANT,
+                       precision="fp64" if prec.startswith("fp64") else prec, **kw)
+    if prec == "fp64-p32":
+        s.set_fp32_preconditioner(True)
+    return s
 
 
 def profile_kernels(solver, wl, bufs, stream):
@@ -529,15 +541,14 @@ def precision_times(torch, dev, B, prec, wl, args, flush, stream):
     `prec` on the workload (inputs resident, timed like the headline), and
     each form's device time per kernel group ({"fused": ..., "plain": ...})."""
     import gato_b200
-    dt = torch.float64 if prec == "fp64" else torch.float32
+    dt = torch.float64 if prec.startswith("fp64") else torch.float32
     T = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
     d_xu0, d_xs, d_goal = T(wl["xu"]), T(wl["xs"]), T(wl["goal"])
     bufs = (d_xu0.clone(), d_xs, d_goal, d_xu0)
     out = []
     kern = {}
     for form in ("fused", "plain"):
-        s = gato_b200.BSQP(batch_size=B, N=N, dt=DT, plant_type=PLANT, form=form,
-                           precision=prec, **solver_kwargs())
+        s = new_solver(prec, B, form=form, **solver_kwargs())
         steps = args.steps if form == "fused" else max(3, args.steps // 2)
         out.append(float(np.mean(time_device_steps(torch, s, bufs, wl, steps, max(1, args.warmup),
                                                    flush, stream))))
@@ -617,9 +628,8 @@ def accuracy_block(wl, sample, threads, xo, so):
     xs, goal = wl["xs"][:sample], wl["goal"][:sample]
 
     def gpu(prec, kwx=None, n=sample):
-        s = gato_b200.BSQP(batch_size=n, N=N, dt=DT, plant_type=PLANT, form="fused",
-                           precision=prec, **dict(solver_kwargs(), **(kwx or {})))
-        f = np.float64 if prec == "fp64" else np.float32
+        s = new_solver(prec, n, form="fused", **dict(solver_kwargs(), **(kwx or {})))
+        f = np.float64 if prec.startswith("fp64") else np.float32
         s.set_lambda(wl["lam"][:n].astype(f))
         s.reset_rho()
         g = s.solve_raw(wl["xu"][:n].astype(f), DT, xs[:n].astype(f), goal[:n].astype(f))
@@ -682,7 +692,8 @@ def _rel_err(a, b):
     return float(np.abs(np.asarray(a) - b).max() / max(1e-12, np.abs(b).max()))
 
 
-def adjoint_config4(torch, dev, threads, precisions=PRECISIONS, B=ADJ_B, fd_problems=ADJ_FD):
+def adjoint_config4(torch, dev, threads, precisions=("fp32", "mixed", "fp64"), B=ADJ_B,
+                    fd_problems=ADJ_FD):
     """Per precision: device times of the forward solve and the adjoint, and
     each gradient's relative error (max |g - g_dense| / max |g_dense| per
     problem; median and max over problems) against the dense FP64 gradient
@@ -1051,9 +1062,8 @@ def run_ours(args):
         line["accuracy_vs_fp64_oracle"] = accuracy
         line["adjoint_config4"] = adj4
         # the fastest form whose trajectories meet the 1e-4 bound against the
-        # oracle on this workload (median and 90th percentile of all problems)
-        ok = [p for p in PRECISIONS if accuracy[p]["xu_rel_err_median"] <= 1e-4 and
-              accuracy[p]["xu_rel_err_p90"] <= 1e-4]
+        # oracle on this workload, every problem (the largest error)
+        ok = [p for p in PRECISIONS if accuracy[p]["xu_rel_err_max"] <= 1e-4]
         if ok:
             best = max(ok, key=lambda p: by_prec[p]["value"])
             line["at_1e-4"] = {"precision": best, "form": "fused (CUDA graph)",

@@ -123,6 +123,7 @@ SIGNATURES = {
     "gato_stage_pcg": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gato_set_cost_diag_batch": (ctypes.c_int, [_vp, _vp]),
     "gato_set_cost_diag_batch_f64": (ctypes.c_int, [_vp, _vp]),
+    "gato_set_fp32_preconditioner": (ctypes.c_int, [_vp, ctypes.c_int]),
     "gato_rollout": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gato_rollout_backward": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp,
                                              _vp, _vp, _vp, _vp, ctypes.c_double,

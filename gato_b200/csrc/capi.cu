@@ -253,6 +253,17 @@ int gato_profile_solve_f64(gato_solver_t* s, void* stream, double* d_xu, const d
     return profile_any(s, stream, d_xu, d_xs, d_goal, ms_by_kernel, launches_by_kernel);
 }
 
+int gato_set_fp32_preconditioner(gato_solver_t* s, int enabled)
+{
+    RC(check_handle(s));
+    RC(check_double(s));
+    if ((enabled != 0) != (s->p32 != 0)) {
+        s->p32 = enabled != 0;
+        s->version++;
+    }
+    return GATO_OK;
+}
+
 int gato_set_wait_limits(gato_solver_t* s, int copy_tries, int step_copy_tries)
 {
     RC(check_handle(s));

@@ -602,6 +602,11 @@ struct RowPcg {
         if (!pcg_p_in_smem<T>()) return base;
         return base + 16 + (size_t)N * n * RD * sizeof(double);
     }
+    // FP64 with the FP32 preconditioner: also the FP32 residual window
+    __host__ __device__ static size_t smem_bytes_p32(int N)
+    {
+        return smem_bytes<double>(N) + 16 + (size_t)(N + 2) * VS * sizeof(float);
+    }
 };
 
 // The RPT rows of S or P^-1 a thread holds in registers.  FP32 rows are kept
@@ -801,13 +806,54 @@ struct NoDzStage {
 // A_k and Qi_k blocks in shared memory, used by the step recovery on the
 // threads where dz_ready() returns true (each thread decides for itself; no
 // barrier depends on it), else read from global memory.
+// P^-1 in FP32 in shared memory for an FP64 PCG (the FP32-preconditioner
+// variant): the same row-major rows, applied to an FP32 copy of the residual
+// window with FP32 FMAs, the row sums returned in FP64.  P^-1 only steers the
+// CG iteration; the system S, the residual, the inner products and the
+// recurrence stay FP64.  Half the shared-memory bytes of the FP64 rows.
+template <int NQ, int RPT>
+struct SmemRowsF {
+    static constexpr int n = 2 * NQ, RD = 3 * n, TPB = n / RPT;
+    const float* base;
+    int row0;
+};
+
+template <int NQ, int RPT>
+__device__ __forceinline__ void rows_window_dot(const SmemRowsF<NQ, RPT>& p, const float* win,
+                                                double (&out)[RPT])
+{
+    constexpr int n = 2 * NQ, VS = row_vs(n), TPB = n / RPT, RD = 3 * n;
+    float acc[RPT][4];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j)
+#pragma unroll
+        for (int a = 0; a < 4; ++a) acc[j][a] = 0.f;
+#pragma unroll
+    for (int blk = 0; blk < 3; ++blk) {
+#pragma unroll
+        for (int c0 = 0; c0 < n; c0 += 2) {
+            const float2 v = *reinterpret_cast<const float2*>(win + blk * VS + c0);
+#pragma unroll
+            for (int j = 0; j < RPT; ++j) {
+                const float2 mm = *reinterpret_cast<const float2*>(
+                    p.base + (size_t)(p.row0 + j * TPB) * RD + blk * n + c0);
+                acc[j][c0 & 3] = fmaf(mm.x, v.x, acc[j][c0 & 3]);
+                acc[j][(c0 + 1) & 3] = fmaf(mm.y, v.y, acc[j][(c0 + 1) & 3]);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < RPT; ++j)
+        out[j] = (double)((acc[j][0] + acc[j][1]) + (acc[j][2] + acc[j][3]));
+}
+
 // PSM: P^-1 in shared memory (SmemRows, FP64), S in registers.  An FP64
 // problem's S and P^-1 (2 x 150 KB for iiwa14 N = 32) do not fit one SM's
 // registers together; the FP64 form with both in registers (one row a
 // thread) spilled and ran the PCG in 10.8 ms per solve (iiwa14 N = 32,
 // 1024 problems), this one in 8.3.
 template <int NQ, typename T, typename Acc, int RPT, class Hook = NoHook,
-          class DzReady = NoDzStage, bool PSM = pcg_p_in_smem<T>()>
+          class DzReady = NoDzStage, bool PSM = pcg_p_in_smem<T>(), bool P32 = false>
 __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int it_row,
                                               unsigned char* smem_raw, const T* Sp = nullptr,
                                               const T* Pp = nullptr, Hook hook = Hook(),
@@ -844,6 +890,14 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
         return true;
     };
     for (int j = tid; j < 2 * L; j += blockDim.x) pv[j] = T(0);
+    // P32: the FP32 copy of the residual window, after the matrix buffer
+    static_assert(!P32 || PSM, "the FP32 preconditioner is a form of the shared-memory P^-1");
+    float* rvf = reinterpret_cast<float*>(
+        ((uintptr_t)(reinterpret_cast<T*>(((uintptr_t)(red + 2 * WARP) + 15) & ~(uintptr_t)15) +
+                     d.b3d()) + 15) & ~(uintptr_t)15);
+    if constexpr (P32) {
+        for (int j = tid; j < L; j += blockDim.x) rvf[j] = 0.f;
+    }
     T* lam = bt.lambda + (size_t)b * d.vecp();
     const int w0 = k * VS;
     int iters = 0;
@@ -860,7 +914,9 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
         // problem.
         static_assert(!PSM || sizeof(T) == 8, "P^-1 in shared memory is FP64");
         RowMat<NQ, RPT, T> srow;
-        std::conditional_t<PSM, SmemRows<NQ, RPT>, RowMat<NQ, RPT, T>> prow;
+        std::conditional_t<P32, SmemRowsF<NQ, RPT>,
+                           std::conditional_t<PSM, SmemRows<NQ, RPT>, RowMat<NQ, RPT, T>>>
+            prow;
         {
             const size_t row = (size_t)(k * n + i0) * RD;
             const size_t prob = (size_t)b * d.b3d();
@@ -879,12 +935,31 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
                 if (!stage_wait(0)) return;
                 srow.load(buf + row, (size_t)TPB * RD, act);
                 __syncthreads();  // every S read of the buffer is done
-                if (tid == 0) {
-                    fence_proxy_async_shared();
-                    mbar_arrive_expect_tx(&s_pbar, bytes);
-                    bulk_copy_g2s(buf, Pg, bytes, &s_pbar);
+                if constexpr (P32) {
+                    // P^-1 in two halves: each bulk-copied into the buffer's
+                    // upper half, then rounded to FP32 into its lower half
+                    const size_t half = d.b3d() / 2;
+                    float* pf = reinterpret_cast<float*>(buf);
+                    for (int h = 0; h < 2; ++h) {
+                        if (tid == 0) {
+                            fence_proxy_async_shared();
+                            mbar_arrive_expect_tx(&s_pbar, bytes / 2);
+                            bulk_copy_g2s(buf + half, Pg + h * half, bytes / 2, &s_pbar);
+                        }
+                        if (!stage_wait(h == 0 ? 1 : 0)) return;
+                        for (size_t e = tid; e < half; e += blockDim.x)
+                            pf[h * half + e] = (float)buf[half + e];
+                        __syncthreads();  // the upper half is read before it is refilled
+                    }
+                    prow.base = pf;
+                } else {
+                    if (tid == 0) {
+                        fence_proxy_async_shared();
+                        mbar_arrive_expect_tx(&s_pbar, bytes);
+                        bulk_copy_g2s(buf, Pg, bytes, &s_pbar);
+                    }
+                    prow.base = buf;
                 }
-                prow.base = buf;
                 prow.row0 = k * n + i0;
             } else {
                 srow.load(Sg + row, (size_t)TPB * RD, act);
@@ -906,14 +981,20 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
 #pragma unroll
         for (int j = 0; j < RPT; ++j) {
             r[j] = act ? g[j] - r[j] : T(0);
-            if (act) rv[(k + 1) * VS + i0 + j * TPB] = r[j];
+            if (act) {
+                rv[(k + 1) * VS + i0 + j * TPB] = r[j];
+                if constexpr (P32) rvf[(k + 1) * VS + i0 + j * TPB] = (float)r[j];
+            }
         }
-        if constexpr (PSM) {
+        if constexpr (PSM && !P32) {
             if (!stage_wait(1)) return;  // P^-1 landed (the wait is also the barrier)
         } else {
             __syncthreads();
         }
-        rows_window_dot(prow, rv + w0, z);
+        if constexpr (P32)
+            rows_window_dot(prow, rvf + w0, z);
+        else
+            rows_window_dot(prow, rv + w0, z);
         const Acc abs_tol = Acc(bt.abs_tol);
         const T eps = bt.tol[b];
         if constexpr (sizeof(T) == 4) {
@@ -1020,10 +1101,16 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
                     for (int j = 0; j < RPT; ++j) {
                         x[j] += alpha * p[j];
                         r[j] -= alpha * ap[j];
-                        if (act) rv[(k + 1) * VS + i0 + j * TPB] = r[j];
+                        if (act) {
+                            rv[(k + 1) * VS + i0 + j * TPB] = r[j];
+                            if constexpr (P32) rvf[(k + 1) * VS + i0 + j * TPB] = (float)r[j];
+                        }
                     }
                     __syncthreads();
-                    rows_window_dot(prow, rv + w0, z);
+                    if constexpr (P32)
+                        rows_window_dot(prow, rvf + w0, z);
+                    else
+                        rows_window_dot(prow, rv + w0, z);
                     part = 0;
 #pragma unroll
                     for (int j = 0; j < RPT; ++j) part += act ? (Acc)r[j] * (Acc)z[j] : Acc(0);
@@ -1129,6 +1216,16 @@ __global__ void __launch_bounds__(RowPcg<NQ, RPT>::MAX_THREADS, 1)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     pcg_rows_body<NQ, T, Acc, RPT>(bt, blockIdx.x, it_row, smem_raw);
+}
+
+// FP64 k_pcg_rows with P^-1 applied in FP32 (gato_set_fp32_preconditioner)
+template <int NQ>
+__global__ void __launch_bounds__(RowPcg<NQ, 2>::MAX_THREADS, 1)
+    k_pcg_rows_p32(Batch<NQ, double> bt, int it_row)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    pcg_rows_body<NQ, double, double, 2, NoHook, NoDzStage, true, true>(bt, blockIdx.x, it_row,
+                                                                         smem_raw);
 }
 
 // Persistent FP32 form of k_pcg_rows: one CTA per SM takes problems from a

@@ -195,6 +195,7 @@ struct gato_solver {
         *ls_count = nullptr, *h_pcg = nullptr, *status = nullptr;
     int* work = nullptr;  // [4]: counters and wait flag of the persistent PCG
     int wait_tries = PCG_STAGE_WAIT_TRIES, wait_tries_dz = PCG_STAGE_WAIT_TRIES;
+    int p32 = 0;  // FP64 solvers: apply P^-1 in FP32 (gato_set_fp32_preconditioner)
     float *h_ls_min = nullptr, *h_ls_step = nullptr;
     // adjoint work buffers, allocated by the first gato_adjoint call
     void *adj_lam = nullptr, *adj_mu = nullptr, *adj_v = nullptr, *adj_scale = nullptr,
@@ -528,6 +529,13 @@ void launch_pcg_rows(gato_solver* s, cudaStream_t st, const Batch<Tg::NQ, typena
         }
     }
     constexpr int RPT = pcg_rows_per_thread<T>();
+    if constexpr (sizeof(T) == 8) {
+        if (s->p32) {
+            k_pcg_rows_p32<NQ><<<s->B, RowPcg<NQ, RPT>::threads(s->N),
+                                 RowPcg<NQ, RPT>::smem_bytes_p32(s->N), st>>>(bt, row);
+            return;
+        }
+    }
     k_pcg_rows<NQ, T, Acc, RPT><<<s->B, RowPcg<NQ, RPT>::threads(s->N),
                                    RowPcg<NQ, RPT>::template smem_bytes<T>(s->N), st>>>(bt, row);
 }
@@ -665,9 +673,12 @@ int configure_kernels(gato_solver* s)
     RC(set_smem(k_fused_kkt<NQ, T, Acc>, lay.bytes(), s->max_smem));
     RC(set_smem(k_fused_schur<NQ, T, Acc>, lay.bytes(), s->max_smem));
     constexpr int RPT = pcg_rows_per_thread<T>();
-    if (rows_pcg_fits<NQ, T>(s->N))  // longer horizons take the cluster PCG
+    if (rows_pcg_fits<NQ, T>(s->N)) {  // longer horizons take the cluster PCG
         RC(set_smem(k_pcg_rows<NQ, T, Acc, RPT>, RowPcg<NQ, RPT>::template smem_bytes<T>(s->N),
                     s->max_smem));
+        if constexpr (sizeof(T) == 8)
+            RC(set_smem(k_pcg_rows_p32<NQ>, RowPcg<NQ, RPT>::smem_bytes_p32(s->N), s->max_smem));
+    }
     if constexpr (sizeof(T) == 4) {
         if (pcg_stream_fits<Tg>(s))
             RC(set_smem(k_pcg_rows_stream<NQ, Acc>,

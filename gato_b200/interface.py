@@ -328,6 +328,12 @@ class BSQP:
         rd = np.full((B, self.nu), self.params.u_cost, np.float32)
         return qd, rd
 
+    def set_fp32_preconditioner(self, enabled=True):
+        """FP64 solvers: apply P^-1 in FP32 inside the FP64 PCG
+        (gato_set_fp32_preconditioner); S, residuals, inner products and the
+        recurrence stay FP64."""
+        L.check(L.load().gato_set_fp32_preconditioner(self._h, int(bool(enabled))))
+
     def set_wait_limits(self, copy_tries=-1, step_copy_tries=-1):
         """Bounds of the persistent PCG's device waits for its bulk copies
         (gato_set_wait_limits): -1 restores the default, 0 gives up at once

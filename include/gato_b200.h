@@ -267,6 +267,16 @@ int gato_set_dt(gato_solver_t* s, float dt);
    is how the tests exercise this path. */
 int gato_set_wait_limits(gato_solver_t* s, int copy_tries, int step_copy_tries);
 
+/* FP64 solvers only (no counterpart in the reference): nonzero applies the
+   preconditioner P^-1 in FP32 inside the FP64 PCG (its rows rounded to FP32
+   in shared memory, applied to an FP32 copy of the residual) while S, the
+   residual, every inner product and the CG recurrence stay FP64.  P^-1 only
+   steers the iteration, so the solution keeps FP64's accuracy up to where
+   the PCG stops; iteration counts can differ from the FP64 oracle's where its
+   stop is marginal.  Horizons that use the cluster PCG (N > 36 for iiwa14)
+   are unaffected.  Default off. */
+int gato_set_fp32_preconditioner(gato_solver_t* s, int enabled);
+
 /* Zeroes the dual warm start.  Replaces BSQP::reset_dual (bsqp.cuh:85). */
 int gato_reset_dual(gato_solver_t* s);
 /* Restores rho and drho to their reset defaults.  Replaces BSQP::reset_rho
