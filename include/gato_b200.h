@@ -273,8 +273,10 @@ int gato_set_wait_limits(gato_solver_t* s, int copy_tries, int step_copy_tries);
    residual, every inner product and the CG recurrence stay FP64.  P^-1 only
    steers the iteration, so the solution keeps FP64's accuracy up to where
    the PCG stops; iteration counts can differ from the FP64 oracle's where its
-   stop is marginal.  Horizons that use the cluster PCG (N > 36 for iiwa14)
-   are unaffected.  Default off. */
+   stop is marginal.  It applies where the one-CTA-per-problem PCG runs (the
+   fused form, gato_adjoint, gato_qp_step_f64, up to N = 36 for iiwa14 and 42
+   for indy7); the plain form's PCG and the cluster PCG of longer horizons are
+   unaffected.  Default off. */
 int gato_set_fp32_preconditioner(gato_solver_t* s, int enabled);
 
 /* Zeroes the dual warm start.  Replaces BSQP::reset_dual (bsqp.cuh:85). */
