@@ -593,19 +593,52 @@ struct RowPcg {
     static constexpr int MAX_THREADS = 512 / RPT;
     __host__ __device__ static int threads(int N) { return ((N * TPB + 31) / 32) * 32; }
     __host__ __device__ static bool fits(int N) { return N * TPB <= MAX_THREADS; }
-    // the two CG vectors and the reduction slots; in FP64 also P^-1
-    // (SmemRows, pcg_p_in_smem)
+    // P^-1 in shared memory (SmemRows, SmemRowsF): block row k starts at
+    // element k * bstride<E>(), a pad after each block row's n x 3n elements.
+    // A lane loads column pairs (2 E) of its rows; the lanes of one
+    // shared-memory wavefront (8 for 16-byte loads, 16 for 8-byte) take
+    // consecutive rows of a block row and then the first rows of the next.
+    // A row is 3n/2 pairs; when that is odd, consecutive rows fall in
+    // distinct banks, and the pad makes the next block row continue that
+    // sequence, so a wavefront's loads never share a bank (unpadded, rows 8
+    // apart collided and every FP64 row load took two wavefronts).
+    template <typename E>
+    __host__ __device__ static constexpr int ppad()
+    {
+        constexpr int W = 128 / (2 * (int)sizeof(E)), s = RD / 2;
+        return (s % 2) ? ((((TPB - n) * s) % W + W) % W) * 2 : 0;
+    }
+    template <typename E>
+    __host__ __device__ static constexpr int bstride()
+    {
+        return n * RD + ppad<E>();
+    }
+    // the FP64 PCG's matrix buffer: S (one copy, unpadded), then P^-1
+    // (padded); with p32 P^-1 in FP32 (padded) and a staging area for half
+    // of the FP64 P^-1 after it
+    __host__ __device__ static size_t psm_buf_bytes(int N, bool p32)
+    {
+        const size_t s_bytes = (size_t)N * n * RD * sizeof(double);
+        size_t p_bytes = (size_t)N * bstride<double>() * sizeof(double);
+        if (p32)
+            p_bytes = (((size_t)N * bstride<float>() * sizeof(float) + 15) & ~(size_t)15) +
+                      s_bytes / 2;
+        return s_bytes > p_bytes ? s_bytes : p_bytes;
+    }
+    // the two CG vectors and the reduction slots; in FP64 also the matrix
+    // buffer (pcg_p_in_smem)
     template <typename T>
     __host__ __device__ static size_t smem_bytes(int N)
     {
         const size_t base = 2 * (size_t)(N + 2) * VS * sizeof(T) + 2 * WARP * sizeof(double) + 16;
         if (!pcg_p_in_smem<T>()) return base;
-        return base + 16 + (size_t)N * n * RD * sizeof(double);
+        return base + 16 + psm_buf_bytes(N, false);
     }
-    // FP64 with the FP32 preconditioner: also the FP32 residual window
+    // FP64 with the FP32 preconditioner: its buffer and the FP32 residual window
     __host__ __device__ static size_t smem_bytes_p32(int N)
     {
-        return smem_bytes<double>(N) + 16 + (size_t)(N + 2) * VS * sizeof(float);
+        const size_t base = 2 * (size_t)(N + 2) * VS * sizeof(double) + 2 * WARP * sizeof(double) + 16;
+        return base + 16 + psm_buf_bytes(N, true) + 16 + (size_t)(N + 2) * VS * sizeof(float);
     }
 };
 
@@ -707,10 +740,10 @@ __device__ __forceinline__ void rows_window_dot(const RowMat<NQ, RPT, float>& ro
 // FP64 P^-1 in shared memory.  An FP64 problem's S and P^-1 (2 x 150 KB for
 // iiwa14 N = 32) do not fit in one SM's registers together: S stays in
 // registers (RPT rows a thread) and P^-1 is bulk-copied into shared memory
-// in its global layout, row-major [N n][3n].  A row is 3n doubles = 21
-// sixteen-byte chunks for iiwa14 (an odd count), so the 16-byte loads of
-// eight threads on consecutive rows fall in eight different bank quads.  The
-// dot product keeps the register form's four partial sums by column mod 4
+// row-major, [N n][3n] with a pad after each block row (RowPcg::bstride): a
+// row is 3n doubles = 21 sixteen-byte chunks for iiwa14 (an odd count), so
+// the 16-byte loads of eight threads on consecutive rows fall in eight
+// different bank quads, across a block-row boundary too.  The dot product keeps the register form's four partial sums by column mod 4
 // and reads each window value once for the thread's RPT rows, so the iterates
 // are those of the register form bit for bit.
 // horizons whose PCG runs k_pcg_rows (one CTA a problem); longer ones take
@@ -724,8 +757,8 @@ __host__ __device__ bool rows_pcg_fits(int N)
 template <int NQ, int RPT>
 struct SmemRows {
     static constexpr int n = 2 * NQ, RD = 3 * n, TPB = n / RPT;
-    const double* base;  // the problem's P^-1 in shared memory
-    int row0;            // the thread's rows: row0 + j * TPB
+    const double* base;  // the thread's first row of P^-1 in shared memory; row j at
+                         // base + j * TPB * RD
 };
 
 template <int NQ, int RPT>
@@ -746,7 +779,7 @@ __device__ __forceinline__ void rows_window_dot(const SmemRows<NQ, RPT>& p, cons
 #pragma unroll
             for (int j = 0; j < RPT; ++j) {
                 const double2 m = *reinterpret_cast<const double2*>(
-                    p.base + (size_t)(p.row0 + j * TPB) * RD + blk * n + c0);
+                    p.base + (size_t)j * TPB * RD + blk * n + c0);
                 acc[j][c0 & 3] += m.x * v.x;
                 acc[j][(c0 + 1) & 3] += m.y * v.y;
             }
@@ -814,8 +847,7 @@ struct NoDzStage {
 template <int NQ, int RPT>
 struct SmemRowsF {
     static constexpr int n = 2 * NQ, RD = 3 * n, TPB = n / RPT;
-    const float* base;
-    int row0;
+    const float* base;  // as SmemRows
 };
 
 template <int NQ, int RPT>
@@ -836,7 +868,7 @@ __device__ __forceinline__ void rows_window_dot(const SmemRowsF<NQ, RPT>& p, con
 #pragma unroll
             for (int j = 0; j < RPT; ++j) {
                 const float2 mm = *reinterpret_cast<const float2*>(
-                    p.base + (size_t)(p.row0 + j * TPB) * RD + blk * n + c0);
+                    p.base + (size_t)j * TPB * RD + blk * n + c0);
                 acc[j][c0 & 3] = fmaf(mm.x, v.x, acc[j][c0 & 3]);
                 acc[j][(c0 + 1) & 3] = fmaf(mm.y, v.y, acc[j][(c0 + 1) & 3]);
             }
@@ -892,9 +924,10 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
     for (int j = tid; j < 2 * L; j += blockDim.x) pv[j] = T(0);
     // P32: the FP32 copy of the residual window, after the matrix buffer
     static_assert(!P32 || PSM, "the FP32 preconditioner is a form of the shared-memory P^-1");
+    unsigned char* mbuf = reinterpret_cast<unsigned char*>(((uintptr_t)(red + 2 * WARP) + 15) &
+                                                           ~(uintptr_t)15);
     float* rvf = reinterpret_cast<float*>(
-        ((uintptr_t)(reinterpret_cast<T*>(((uintptr_t)(red + 2 * WARP) + 15) & ~(uintptr_t)15) +
-                     d.b3d()) + 15) & ~(uintptr_t)15);
+        ((uintptr_t)(mbuf + RP::psm_buf_bytes(N, P32)) + 15) & ~(uintptr_t)15);
     if constexpr (P32) {
         for (int j = tid; j < L; j += blockDim.x) rvf[j] = 0.f;
     }
@@ -923,7 +956,7 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
             const T* Sg = Sp ? Sp : bt.S + prob;
             const T* Pg = Pp ? Pp : bt.P + prob;
             if constexpr (PSM) {
-                T* buf = reinterpret_cast<T*>(((uintptr_t)(red + 2 * WARP) + 15) & ~(uintptr_t)15);
+                T* buf = reinterpret_cast<T*>(mbuf);
                 const uint32_t bytes = (uint32_t)(d.b3d() * sizeof(T));
                 if (tid == 0) {
                     mbar_init(&s_pbar, 1);
@@ -935,32 +968,46 @@ __device__ __forceinline__ void pcg_rows_body(const Batch<NQ, T>& bt, int b, int
                 if (!stage_wait(0)) return;
                 srow.load(buf + row, (size_t)TPB * RD, act);
                 __syncthreads();  // every S read of the buffer is done
+                constexpr int BR = n * RD;  // elements of a block row
                 if constexpr (P32) {
-                    // P^-1 in two halves: each bulk-copied into the buffer's
-                    // upper half, then rounded to FP32 into its lower half
+                    // P^-1 in two halves: each bulk-copied into a staging
+                    // area after the FP32 rows, then rounded to FP32 into
+                    // the padded layout
+                    constexpr int BSF = RP::template bstride<float>();
                     const size_t half = d.b3d() / 2;
                     float* pf = reinterpret_cast<float*>(buf);
+                    T* stg = reinterpret_cast<T*>(
+                        ((uintptr_t)(pf + (size_t)N * BSF) + 15) & ~(uintptr_t)15);
                     for (int h = 0; h < 2; ++h) {
                         if (tid == 0) {
                             fence_proxy_async_shared();
                             mbar_arrive_expect_tx(&s_pbar, bytes / 2);
-                            bulk_copy_g2s(buf + half, Pg + h * half, bytes / 2, &s_pbar);
+                            bulk_copy_g2s(stg, Pg + h * half, bytes / 2, &s_pbar);
                         }
                         if (!stage_wait(h == 0 ? 1 : 0)) return;
-                        for (size_t e = tid; e < half; e += blockDim.x)
-                            pf[h * half + e] = (float)buf[half + e];
-                        __syncthreads();  // the upper half is read before it is refilled
+                        for (size_t e = tid; e < half; e += blockDim.x) {
+                            const size_t idx = h * half + e;
+                            const size_t kb = idx / BR;
+                            pf[kb * BSF + (idx - kb * BR)] = (float)stg[e];
+                        }
+                        __syncthreads();  // the staging area is read before it is refilled
                     }
-                    prow.base = pf;
+                    prow.base = pf + (size_t)k * BSF + i0 * RD;
                 } else {
+                    constexpr int BS = RP::template bstride<double>();
                     if (tid == 0) {
                         fence_proxy_async_shared();
                         mbar_arrive_expect_tx(&s_pbar, bytes);
-                        bulk_copy_g2s(buf, Pg, bytes, &s_pbar);
+                        if constexpr (BS == BR) {
+                            bulk_copy_g2s(buf, Pg, bytes, &s_pbar);
+                        } else {
+                            for (int kb = 0; kb < N; ++kb)  // one copy a block row
+                                bulk_copy_g2s(buf + (size_t)kb * BS, Pg + (size_t)kb * BR,
+                                              (uint32_t)(BR * sizeof(T)), &s_pbar);
+                        }
                     }
-                    prow.base = buf;
+                    prow.base = buf + (size_t)k * BS + i0 * RD;
                 }
-                prow.row0 = k * n + i0;
             } else {
                 srow.load(Sg + row, (size_t)TPB * RD, act);
                 prow.load(Pg + row, (size_t)TPB * RD, act);
