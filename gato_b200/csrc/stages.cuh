@@ -298,19 +298,62 @@ __device__ void schur_knot(int k, T rho, const T* __restrict__ Qi,
     using L = SchurSmem<NQ>;
     constexpr int n = L::n, m = L::m, n2 = L::n2, RD = 3 * n;
     const int l = lane_id();
-    for (int i = l; i < n2; i += WARP) {
-        s[L::A + i] = A[k * n2 + i];
-        s[L::QI + i] = Qi[k * n2 + i];
-        s[L::QI1 + i] = Qi[(k + 1) * n2 + i];
+    // every global load of the knot is issued before the first store to
+    // shared memory, so the warp waits for one round trip, not one per
+    // strided pass
+    constexpr int P2 = (n2 + WARP - 1) / WARP, PB = (n * m + WARP - 1) / WARP,
+                  PR = (m * m + WARP - 1) / WARP;
+    T ga[P2], gq[P2], gq1[P2], gb[PB], gr[PR], gv[4];
+#pragma unroll
+    for (int it = 0; it < P2; ++it) {
+        const int i = l + it * WARP;
+        if (i < n2) {
+            ga[it] = A[k * n2 + i];
+            gq[it] = Qi[k * n2 + i];
+            gq1[it] = Qi[(k + 1) * n2 + i];
+        }
     }
-    for (int i = l; i < n * m; i += WARP) s[L::B + i] = Bm[k * n * m + i];
-    for (int i = l; i < m * m; i += WARP) s[L::RI + i] = Ri[k * m * m + i];
+#pragma unroll
+    for (int it = 0; it < PB; ++it) {
+        const int i = l + it * WARP;
+        if (i < n * m) gb[it] = Bm[k * n * m + i];
+    }
+#pragma unroll
+    for (int it = 0; it < PR; ++it) {
+        const int i = l + it * WARP;
+        if (i < m * m) gr[it] = Ri[k * m * m + i];
+    }
     if (l < n) {
-        s[L::V + l] = qv[k * n + l];
-        s[L::V + n + l] = qv[(k + 1) * n + l];
-        s[L::V + 2 * n + m + l] = c[(k + 1) * n + l];
+        gv[0] = qv[k * n + l];
+        gv[1] = qv[(k + 1) * n + l];
+        gv[2] = c[(k + 1) * n + l];
     }
-    if (l < m) s[L::V + 2 * n + l] = rv[k * m + l];
+    if (l < m) gv[3] = rv[k * m + l];
+#pragma unroll
+    for (int it = 0; it < P2; ++it) {
+        const int i = l + it * WARP;
+        if (i < n2) {
+            s[L::A + i] = ga[it];
+            s[L::QI + i] = gq[it];
+            s[L::QI1 + i] = gq1[it];
+        }
+    }
+#pragma unroll
+    for (int it = 0; it < PB; ++it) {
+        const int i = l + it * WARP;
+        if (i < n * m) s[L::B + i] = gb[it];
+    }
+#pragma unroll
+    for (int it = 0; it < PR; ++it) {
+        const int i = l + it * WARP;
+        if (i < m * m) s[L::RI + i] = gr[it];
+    }
+    if (l < n) {
+        s[L::V + l] = gv[0];
+        s[L::V + n + l] = gv[1];
+        s[L::V + 2 * n + m + l] = gv[2];
+    }
+    if (l < m) s[L::V + 2 * n + l] = gv[3];
     __syncwarp();
     // phi = A Qi_k, BRi = B Ri, theta = Qi_{k+1} + phi A^T + BRi B^T
     warp_gemm<n, n, n, false, false, T>(s + L::PHI, s + L::A, s + L::QI);
@@ -389,11 +432,27 @@ __device__ void schur_offdiag(int k, const T* __restrict__ S, T* __restrict__ P,
     const T* Pa = P + (k + 1) * 3 * n2 + n;
     const T* Pb = P + k * 3 * n2 + n;
     const T* Sl = S + (k + 1) * 3 * n2;
-    for (int i = l; i < n2; i += WARP) {
-        const int y = i / n, x = i % n;
-        Ta[x * n + y] = Pa[y * RD + x];
-        Tb[x * n + y] = Pb[y * RD + x];
-        ph[x * n + y] = Sl[y * RD + x];
+    constexpr int P2 = (n2 + WARP - 1) / WARP;
+    T ga[P2], gb[P2], gp[P2];  // all loads first, as in schur_knot
+#pragma unroll
+    for (int it = 0; it < P2; ++it) {
+        const int i = l + it * WARP;
+        if (i < n2) {
+            const int y = i / n, x = i % n;
+            ga[it] = Pa[y * RD + x];
+            gb[it] = Pb[y * RD + x];
+            gp[it] = Sl[y * RD + x];
+        }
+    }
+#pragma unroll
+    for (int it = 0; it < P2; ++it) {
+        const int i = l + it * WARP;
+        if (i < n2) {
+            const int y = i / n, x = i % n;
+            Ta[x * n + y] = ga[it];
+            Tb[x * n + y] = gb[it];
+            ph[x * n + y] = gp[it];
+        }
     }
     __syncwarp();
     warp_gemm<n, n, n, false, false, T>(sc, ph, Tb);
