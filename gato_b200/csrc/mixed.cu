@@ -47,7 +47,7 @@ bool rows_fit(const gato_solver* s)
 }
 
 template <typename T, typename Acc, int KG, int PPB, int MINB>
-int launch_q_fused(gato_mixed* mx, cudaStream_t st, const MultiArgs<T>& ma, int it)
+int launch_q_kkt(gato_mixed* mx, cudaStream_t st, const MultiArgs<T>& ma, int it)
 {
     int team_bytes = 0;
     for (int c = 0; c < mx->ncls; ++c) {
@@ -58,7 +58,7 @@ int launch_q_fused(gato_mixed* mx, cudaStream_t st, const MultiArgs<T>& ma, int 
         team_bytes = std::max(team_bytes, (int)((by + 255) & ~(size_t)255));
     }
     const size_t smem = (size_t)PPB * team_bytes;
-    auto kern = k_q_fused_iter<T, Acc, KG, PPB, MINB>;
+    auto kern = k_q_kkt<T, Acc, KG, PPB, MINB>;
     if (smem > 48 * 1024)
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
@@ -69,19 +69,41 @@ int launch_q_fused(gato_mixed* mx, cudaStream_t st, const MultiArgs<T>& ma, int 
     return GATO_OK;
 }
 
+// the Schur half: one problem per CTA, its own queue counter (ma.head)
 template <typename T, typename Acc>
-int launch_q_fused_any(gato_mixed* mx, cudaStream_t st, const MultiArgs<T>& ma, int it)
+int launch_q_schur(gato_mixed* mx, cudaStream_t st, const MultiArgs<T>& ma, int it)
+{
+    size_t smem = 0;
+    for (int c = 0; c < mx->ncls; ++c) {
+        const gato_solver* s = mx->cls[c];
+        const size_t by = s->nq == 7 ? FusedLayout<7, T>{s->N, 8, false}.bytes()
+                                     : FusedLayout<6, T>{s->N, 8, false}.bytes();
+        smem = std::max(smem, by);
+    }
+    auto kern = k_q_schur<T, Acc>;
+    if (smem > 48 * 1024)
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, smem));
+    const int grid = std::max(1, std::min(mx->nsm * std::max(occ, 1), ma.nitems));
+    kern<<<grid, 256, smem, st>>>(ma, it);
+    CKL();
+    return GATO_OK;
+}
+
+template <typename T, typename Acc>
+int launch_q_kkt_any(gato_mixed* mx, cudaStream_t st, const MultiArgs<T>& ma, int it)
 {
     const int sel = (mx->kg == 32 ? 4 : 0) + (mx->ppb == 2 ? 2 : 0) + (mx->occ == 4 ? 1 : 0);
     switch (sel) {
-        case 0: return launch_q_fused<T, Acc, 16, 1, 2>(mx, st, ma, it);
-        case 1: return launch_q_fused<T, Acc, 16, 1, 4>(mx, st, ma, it);
-        case 2: return launch_q_fused<T, Acc, 16, 2, 2>(mx, st, ma, it);
-        case 3: return launch_q_fused<T, Acc, 16, 2, 4>(mx, st, ma, it);
-        case 4: return launch_q_fused<T, Acc, 32, 1, 2>(mx, st, ma, it);
-        case 5: return launch_q_fused<T, Acc, 32, 1, 4>(mx, st, ma, it);
-        case 6: return launch_q_fused<T, Acc, 32, 2, 2>(mx, st, ma, it);
-        default: return launch_q_fused<T, Acc, 32, 2, 4>(mx, st, ma, it);
+        case 0: return launch_q_kkt<T, Acc, 16, 1, 2>(mx, st, ma, it);
+        case 1: return launch_q_kkt<T, Acc, 16, 1, 4>(mx, st, ma, it);
+        case 2: return launch_q_kkt<T, Acc, 16, 2, 2>(mx, st, ma, it);
+        case 3: return launch_q_kkt<T, Acc, 16, 2, 4>(mx, st, ma, it);
+        case 4: return launch_q_kkt<T, Acc, 32, 1, 2>(mx, st, ma, it);
+        case 5: return launch_q_kkt<T, Acc, 32, 1, 4>(mx, st, ma, it);
+        case 6: return launch_q_kkt<T, Acc, 32, 2, 2>(mx, st, ma, it);
+        default: return launch_q_kkt<T, Acc, 32, 2, 4>(mx, st, ma, it);
     }
 }
 
@@ -139,7 +161,8 @@ int enqueue_mixed(gato_mixed* mx, cudaStream_t st, void* const* xu, const void* 
     k_q_merit_ls<T, Acc><<<grid_m, 256, merit_smem, st>>>(queue(mx->d_items, mx->nitems), 0, 0);
     CKL();
     for (int it = 0; it < iters; ++it) {
-        RC((launch_q_fused_any<T, Acc>(mx, st, queue(mx->d_items, mx->nitems), it)));
+        RC((launch_q_kkt_any<T, Acc>(mx, st, queue(mx->d_items, mx->nitems), it)));
+        RC((launch_q_schur<T, Acc>(mx, st, queue(mx->d_items, mx->nitems), it)));
         if (has_long) {
             CK(cudaEventRecord(mx->fork, st));
             CK(cudaStreamWaitEvent(mx->side, mx->fork, 0));
@@ -288,7 +311,7 @@ int gato_mixed_create(const gato_class_t* classes, int nclasses, const gato_para
         }
     mx->nitems = (int)all.size();
     mx->nrows = (int)rows.size();
-    mx->nheads = 3 * std::max(1, params->max_sqp_iters) + 2;
+    mx->nheads = 4 * std::max(1, params->max_sqp_iters) + 2;  // KKT, Schur, PCG, merit per iteration
     int err = GATO_OK;
     auto ck = [&](cudaError_t e) {
         if (e != cudaSuccess && !err) err = fail(GATO_ERR_CUDA, "%s", cudaGetErrorString(e));

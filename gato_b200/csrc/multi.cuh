@@ -42,14 +42,13 @@ __device__ __forceinline__ int queue_next(int* head, int nitems, int* s_item)
     return queue_next(head, nitems, s_item, Team::cta());
 }
 
-// KKT + Schur system of every queued problem (S, P^-1, gamma to global
-// memory).  KG lanes per knot; PPB problems per CTA at a time (the CTA's
-// warps split into PPB teams that pull work independently, each with
-// team_bytes of shared memory); MINB CTAs per SM in FP32 (registers traded
-// for resident warps).
+// KKT blocks of every queued problem (to global memory).  KG lanes per knot;
+// PPB problems per CTA at a time (the CTA's warps split into PPB teams that
+// pull work independently, each with team_bytes of shared memory); MINB
+// CTAs per SM in FP32 (registers traded for resident warps).
 template <typename T, typename Acc, int KG, int PPB, int MINB>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MINB : 1)
-    k_q_fused_iter(MultiArgs<T> ma, int it_row, int team_bytes)
+    k_q_kkt(MultiArgs<T> ma, int it_row, int team_bytes)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_item[PPB];
@@ -61,9 +60,35 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? MINB : 1)
         if (it < 0) break;
         const int2 w = ma.items[it];
         if (ma.nq[w.x] == 7)
-            fused_iter_body<7, T, Acc, KG>(ma.b7[w.x], ma.m7, w.y, 0, it_row, 0, sm, team);
+            fused_iter_body<7, T, Acc, KG, true, false>(ma.b7[w.x], ma.m7, w.y, 0, it_row, 0, sm,
+                                                        team);
         else
-            fused_iter_body<6, T, Acc, KG>(ma.b6[w.x], ma.m6, w.y, 0, it_row, 0, sm, team);
+            fused_iter_body<6, T, Acc, KG, true, false>(ma.b6[w.x], ma.m6, w.y, 0, it_row, 0, sm,
+                                                        team);
+    }
+}
+
+// Schur system of every queued problem (S, P^-1, gamma to global memory)
+// from the blocks k_q_kkt left there: the two halves of the SQP iteration's
+// set-up as separate launches, each compiled for its own occupancy, as
+// k_fused_kkt and k_fused_schur are for one class (four CTAs per SM in
+// FP32, two in FP64).
+template <typename T, typename Acc>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
+    k_q_schur(MultiArgs<T> ma, int it_row)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_item;
+    for (;;) {
+        const int it = queue_next(ma.head, ma.nitems, &s_item);
+        if (it < 0) break;
+        const int2 w = ma.items[it];
+        if (ma.nq[w.x] == 7)
+            fused_iter_body<7, T, Acc, 16, false, true>(ma.b7[w.x], ma.m7, w.y, 0, it_row, 0,
+                                                        smem_raw, Team::cta(), false);
+        else
+            fused_iter_body<6, T, Acc, 16, false, true>(ma.b6[w.x], ma.m6, w.y, 0, it_row, 0,
+                                                        smem_raw, Team::cta(), false);
     }
 }
 
