@@ -43,9 +43,18 @@ def run_pair(O, plant, N, B, params, form, precision, seed, perturbed=True, goal
 
 @pytest.mark.parametrize("plant,N,form", [("iiwa14", 8, "fused"), ("iiwa14", 32, "fused"),
                                           ("iiwa14", 32, "plain"), ("indy7", 32, "fused"),
-                                          ("iiwa14", 64, "fused"), ("indy7", 128, "fused")])
+                                          ("iiwa14", 64, "fused"), ("indy7", 128, "fused"),
+                                          ("iiwa14", 2, "fused"), ("iiwa14", 36, "fused"),
+                                          ("iiwa14", 37, "fused"), ("indy7", 42, "fused")])
 def test_fp64_solve_reproduces_oracle(oracle_mod, plant, N, form):
-    """N = 64 and 128 run the cluster PCG (block rows split across CTAs)."""
+    """N = 64 and 128 run the cluster PCG (block rows split across CTAs).
+    The horizon edges: N = 2 (one knot pair), the longest horizons of the
+    one-CTA PCG (iiwa14 N = 36, its padded P^-1 the largest shared-memory
+    buffer; indy7 N = 42) and the first cluster horizon (iiwa14 N = 37).
+    lambda is the PCG's iterate, so it is compared at the PCG's relative
+    tolerance (1e-5): with the same iteration count, the two sums' rounding
+    orders leave it up to 3.3e-6 apart (indy7 N = 42), while XU agrees to
+    1e-8."""
     r = run_pair(oracle_mod, plant, N, 4, PARAMS_CFG2, form, "fp64", seed=31)
     g, o = r["g"], r["o"]
     assert g["ls_num_iters"] == o["ls_num_iters"]
@@ -54,7 +63,7 @@ def test_fp64_solve_reproduces_oracle(oracle_mod, plant, N, form):
     np.testing.assert_array_equal(g["kkt_converged"], o["kkt_converged"])
     np.testing.assert_array_equal(g["ls_step_size"], o["ls_step_size"].astype(np.float32))
     assert nerr(g["XU"], r["xo"]) < 1e-8
-    assert nerr(r["lam_g"], r["lam_o"]) < 1e-6
+    assert nerr(r["lam_g"], r["lam_o"]) < PARAMS_CFG2["pcg_tol"]
     np.testing.assert_allclose(g["final_merit"], o["final_merit"], rtol=1e-6)
     np.testing.assert_allclose(r["rho_g"], r["rho_o"], rtol=1e-6)
 
@@ -169,7 +178,7 @@ def test_fp32_stepwise_parity_n32(oracle_mod):
     assert errs and max(errs) < 5e-3 and float(np.median(errs)) < 1e-3, errs
 
 
-@pytest.mark.parametrize("N", [32, 64])
+@pytest.mark.parametrize("N", [2, 32, 36, 64])
 def test_plain_and_fused_forms_agree(N):
     """The fused form evaluates the same stages with differently organised
     kernels (register-resident PCG, sample-per-thread merit), so it rounds
