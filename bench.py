@@ -1341,6 +1341,9 @@ def run_mpc(args):
 # --------------------------------------------------------------------------
 # batch-size sweep of the headline workload (iiwa14 N=32, 5 SQP iterations)
 SWEEP_BATCHES = (1, 32, 128, 512, 1024)
+# this library's arm also runs batches past the headline's, to the sizes an
+# HBM-resident batch reaches (16384 problems: about 13 GB of solver buffers)
+SWEEP_BATCHES_OURS = SWEEP_BATCHES + (4096, 16384)
 
 
 def run_sweep(args):
@@ -1353,7 +1356,7 @@ def run_sweep(args):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.Stream(device=dev)
     rows = []
-    for B in SWEEP_BATCHES:
+    for B in SWEEP_BATCHES_OURS:
         wl = make_workload(B, seed=2026)
         s = gato_b200.BSQP(batch_size=B, N=N, dt=DT, plant_type=PLANT, form="fused", **kw)
         T = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
