@@ -814,12 +814,43 @@ __device__ __forceinline__ void rows_block_sum2(Acc& a, Acc& b, Acc* red)
     __syncthreads();
     Acc sa = 0, sb = 0, ta = 0, tb = 0;  // even and odd warps: half the dependent adds
     const int nw = blockDim.x / WARP;
-    for (int w = 0; w < nw; w += 2) {
-        sa += red[w];
-        sb += red[WARP + w];
-        if (w + 1 < nw) {
-            ta += red[w + 1];
-            tb += red[WARP + w + 1];
+    if (nw <= 8) {
+        // the (up to) eight slots of each sum in 16-byte loads (red is
+        // 16-byte aligned; slots past nw are loaded and not used)
+        Acc ra[8], rb[8];
+#pragma unroll
+        for (int w = 0; w < 8; w += 16 / (int)sizeof(Acc)) {
+            if constexpr (sizeof(Acc) == 4) {
+                const float4 u = *reinterpret_cast<const float4*>(red + w);
+                const float4 v = *reinterpret_cast<const float4*>(red + WARP + w);
+                ra[w] = u.x, ra[w + 1] = u.y, ra[w + 2] = u.z, ra[w + 3] = u.w;
+                rb[w] = v.x, rb[w + 1] = v.y, rb[w + 2] = v.z, rb[w + 3] = v.w;
+            } else {
+                const double2 u = *reinterpret_cast<const double2*>(red + w);
+                const double2 v = *reinterpret_cast<const double2*>(red + WARP + w);
+                ra[w] = u.x, ra[w + 1] = u.y;
+                rb[w] = v.x, rb[w + 1] = v.y;
+            }
+        }
+#pragma unroll
+        for (int w = 0; w < 8; w += 2) {
+            if (w < nw) {
+                sa += ra[w];
+                sb += rb[w];
+            }
+            if (w + 1 < nw) {
+                ta += ra[w + 1];
+                tb += rb[w + 1];
+            }
+        }
+    } else {
+        for (int w = 0; w < nw; w += 2) {
+            sa += red[w];
+            sb += red[WARP + w];
+            if (w + 1 < nw) {
+                ta += red[w + 1];
+                tb += red[WARP + w + 1];
+            }
         }
     }
     a = sa + ta;
